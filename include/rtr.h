@@ -1,0 +1,147 @@
+/* rtr.h -- C ABI of librtr.so, the B200 (sm_100a) implementation of the
+ * RTRExtractor decomposition path: weighted per-edge triangle counting,
+ * cascading edge cleaning and dense-cluster extraction.
+ *
+ * Plain pointers and sizes only.  The library owns all device memory of a
+ * graph; the caller owns every host buffer it passes in.  Every call returns
+ * an rtr_status (0 = RTR_OK); on failure rtr_last_error() describes the cause
+ * (per calling thread).  Nothing in the library calls exit().  Calls on
+ * different graphs may run concurrently from different threads; calls on one
+ * graph must not overlap.
+ *
+ * Array layouts follow the reference:
+ *   offsets  int64[n+1], nbors int64[2m]   the symmetric CSR of makeCSR
+ *                                           (RTRex_Sequential/Graph.cpp:344-384),
+ *                                           rows ascending by neighbour id
+ *   perEdge  double[2m]  one cell per directed slot (both copies of an edge
+ *                        hold the same value), perVertex double[n]
+ *   status   uint8[2m]   'Y' alive / 'N' deleted, as edgeStatus
+ *                        (RTRex_Sequential/Escape/Decomposition.h:127)
+ *   support  uint32[2m]  live triangles on each slot (integer companion)
+ * Inputs must be simple graphs (no self-loops, no repeated pairs) unless
+ * RTR_FLAG_SIMPLIFY is passed, which drops them before building the CSR.
+ */
+#ifndef RTR_H
+#define RTR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rtr_graph rtr_graph;
+
+enum rtr_status {
+    RTR_OK = 0,
+    RTR_ERR_ARG = 1,     /* null pointer / bad argument */
+    RTR_ERR_CUDA = 2,    /* CUDA runtime error or allocation failure */
+    RTR_ERR_INPUT = 3,   /* malformed graph: ids out of range, self-loops, duplicates, asymmetric CSR */
+    RTR_ERR_LIMIT = 4,   /* size beyond the supported index width (n, 2m < 2^31-1) */
+    RTR_ERR_STATE = 5,   /* stage called out of order */
+    RTR_ERR_DEVICE = 6,  /* a kernel reported an internal inconsistency (error word) */
+    RTR_ERR_IO = 7       /* file could not be read or written / short edge count */
+};
+
+enum rtr_flags {
+    RTR_FLAG_SIMPLIFY = 1 /* drop self-loops and duplicate pairs instead of rejecting them */
+};
+
+/* Library version string and the calling thread's last error message. */
+const char* rtr_version(void);
+const char* rtr_last_error(void);
+
+/* Build a graph on `device` from m undirected pairs (src[i], dst[i]), 0 <= id < n,
+ * stored in both directions as loadGraph(.., undirected=1, escape) does, with
+ * the CSR built on the device (radix sort, offsets, partner map).
+ * Replaces: loadGraph_Escape's edge storage (RTRex_Sequential/GraphIO.cpp:42-63),
+ *           makeCSR (RTRex_Sequential/Graph.cpp:344-384),
+ *           CGraph::getPartnerMap (RTRex_Sequential/Graph.cpp:320-340) and
+ *           transferGraphToDevice (RTRex_CUDA/gpu_graph.cuh:47-52). */
+int rtr_graph_create_from_edges(const int64_t* src, const int64_t* dst, int64_t m, int64_t n, int device, int flags,
+                                rtr_graph** out);
+
+/* Build a graph from a host CSR (symmetric, rows strictly ascending).
+ * Replaces: transferGraphToDevice(h_offsets, h_nbors, nVertices, nEdges, dg)
+ *           (RTRex_CUDA/gpu_graph.cuh:47-52) with allocateDeviceState (:57). */
+int rtr_graph_create_from_csr(const int64_t* offsets, const int64_t* nbors, int64_t n, int device, rtr_graph** out);
+
+/* Release every device buffer of the graph.
+ * Replaces: freeDeviceGraph (RTRex_CUDA/gpu_graph.cuh:62). */
+int rtr_graph_destroy(rtr_graph* g);
+
+/* n and the number of undirected edges m (nEdges/2 in the reference). */
+int rtr_graph_info(const rtr_graph* g, int64_t* n, int64_t* m);
+
+/* Weighted triangle counting: perEdge, perVertex, support and the total.
+ * Replaces: commonNbr (RTRex_Sequential/Escape/Decomposition.h:42-117) and
+ *           gpuCommonNbr (RTRex_CUDA/gpu_triangle_count.cuh:23). */
+int rtr_count(rtr_graph* g, int64_t* total_triangles);
+
+/* Initial clean at threshold eps (edges with perEdge < eps/(du*dv) are removed
+ * in cascade); returns the triangles left.
+ * Replaces: initialClean (Decomposition.h:302-460, deleteAndClean :147-283) and
+ *           gpuInitialClean (RTRex_CUDA/gpu_clean.cuh:30). */
+int rtr_clean(rtr_graph* g, double eps, int64_t* triangles_left);
+
+/* Cluster extraction from the cleaned graph; returns the number of clusters.
+ * Replaces: disjointExtract's seed loop (Decomposition.h:566-919) with
+ *           populateStats (:473-491), and disjointExtractCUDA
+ *           (RTRex_CUDA/main.cu:130-338) with gpuExtractInner / gpuMarkClusterEdges /
+ *           gpuDeleteAndClean (RTRex_CUDA/gpu_extract.cuh:28-59, gpu_clean.cuh:44). */
+int rtr_extract(rtr_graph* g, int64_t* n_clusters);
+
+/* rtr_count + rtr_clean(eps) + rtr_extract in one call.
+ * Replaces: disjointExtract (Decomposition.h:538-940). */
+int rtr_decompose(rtr_graph* g, double eps, int64_t* n_clusters);
+
+/* Copy the CSR to host buffers (offsets[n+1], nbors[2m]). */
+int rtr_get_csr(const rtr_graph* g, int64_t* offsets, int64_t* nbors);
+
+/* Copy the current weights (any pointer may be NULL).
+ * Replaces: syncWeightsDeviceToHost (RTRex_CUDA/gpu_graph.cuh:69-73). */
+int rtr_get_weights(const rtr_graph* g, double* perEdge, double* perVertex, uint32_t* support, int64_t* total);
+
+/* Copy the edge status ('Y' / 'N'; 'S' never remains after a stage).
+ * Replaces: syncEdgeStatusDeviceToHost (RTRex_CUDA/gpu_graph.cuh:77). */
+int rtr_get_status(const rtr_graph* g, uint8_t* status);
+
+/* Copy the clusters in creation order: cluster k has seed[k], nVertices nv[k],
+ * internal edges ne[k], cut edges cut[k], and members vert[off[k] .. off[k+1])
+ * in the order the reference's unordered_set iterates them.
+ * Sizes: seed/nv/ne/cut[n_clusters], off[n_clusters+1], vert[n].
+ * Replaces: the vector<Cluster> returned by disjointExtract (Decomposition.h:538). */
+int rtr_get_clusters(const rtr_graph* g, int64_t* seed, int64_t* nv, int64_t* ne, int64_t* cut, int64_t* off,
+                     int64_t* vert);
+
+/* cluster_of[v] = index of v's cluster (creation order), the cluster_map of
+ * disjointExtract (Decomposition.h:538). */
+int rtr_get_cluster_of(const rtr_graph* g, int64_t* cluster_of);
+
+/* Stage times in milliseconds from CUDA events: [build, count, clean, extract];
+ * kernel launches issued for this graph so far; diagnostic counter of the
+ * reference's residual self-check (Decomposition.h:273-277). */
+int rtr_get_stats(const rtr_graph* g, double* ms4, int64_t* launches, int64_t* residual_warnings);
+
+/* Write <name>-decomposition.txt, -stats.txt, -freq.txt and -cut.txt exactly as
+ * printDecomposition does (RTRex_Sequential/clustering/RTRex.cpp:19-118,
+ * RTRex_CUDA/main.cu:57-108), and print its summary lines to stdout. */
+int rtr_write_decomposition(const rtr_graph* g, const char* name);
+
+/* Parse an Escape edge-list file (first data line "n m", then m lines "u v";
+ * '#' and blank lines skipped) into malloc'ed arrays released with rtr_free.
+ * Replaces: loadGraph(path, g, 1, IOFormat::escape) (RTRex_Sequential/GraphIO.cpp:19-88);
+ * returns RTR_ERR_IO when fewer than m edges are present (GraphIO.cpp:67-71). */
+int rtr_load_escape(const char* path, int64_t* n, int64_t* m, int64_t** src, int64_t** dst);
+void rtr_free(void* p);
+
+/* The whole drop-in driver: load, decompose at eps on `device`, and write
+ * <prefix><name>-{decomposition,stats,freq,cut}.txt.
+ * Replaces: RTRex_CUDA main (RTRex_CUDA/main.cu:343-391) with prefix "RTRex-CUDA-",
+ *           and RTRex main's decomposition output (RTRex.cpp:176-194) with "RTRex-". */
+int rtr_run_file(const char* graph_path, const char* name, double eps, int device, const char* prefix, int flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTR_H */

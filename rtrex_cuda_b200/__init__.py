@@ -1,0 +1,266 @@
+"""B200-native RTRExtractor decomposition path.
+
+Python front end over the C ABI of ``librtr.so`` (declared in
+``include/rtr.h``).  The CUDA library is the only compute path: importing
+works without a GPU, but every graph operation goes through librtr.so and
+fails with :class:`RtrError` when no CUDA device is present; there is no CPU
+fallback.
+
+Typical use::
+
+    import rtrex_cuda_b200 as rtr
+    g = rtr.Graph.from_edges(n, src, dst)          # device CSR build
+    total = g.count()                               # commonNbr
+    left = g.clean(0.3)                             # initialClean
+    k = g.extract()                                 # disjointExtract loop
+    clusters = g.clusters()
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+__all__ = ["RtrError", "Graph", "Clusters", "lib", "lib_path", "run_file", "load_escape", "build"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "librtr.so")
+_lib = None
+
+RTR_FLAG_SIMPLIFY = 1
+
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+
+
+class RtrError(RuntimeError):
+    """A librtr call returned a non-zero rtr_status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rtr error {code}: {msg}")
+        self.code = code
+
+
+def lib_path() -> str:
+    return _LIB_PATH
+
+
+def build(verbose: bool = False) -> str:
+    from . import build as _b
+    return _b.build(verbose)
+
+
+def lib():
+    """Load librtr.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise RtrError(-1, f"{_LIB_PATH} is missing; run python -m rtrex_cuda_b200.build")
+    L = ctypes.CDLL(_LIB_PATH)
+    P = ctypes.POINTER
+    L.rtr_version.restype = ctypes.c_char_p
+    L.rtr_last_error.restype = ctypes.c_char_p
+    L.rtr_graph_create_from_edges.argtypes = [_vp, _vp, _i64, _i64, ctypes.c_int, ctypes.c_int, P(_vp)]
+    L.rtr_graph_create_from_csr.argtypes = [_vp, _vp, _i64, ctypes.c_int, P(_vp)]
+    L.rtr_graph_destroy.argtypes = [_vp]
+    L.rtr_graph_info.argtypes = [_vp, P(_i64), P(_i64)]
+    L.rtr_count.argtypes = [_vp, P(_i64)]
+    L.rtr_clean.argtypes = [_vp, ctypes.c_double, P(_i64)]
+    L.rtr_extract.argtypes = [_vp, P(_i64)]
+    L.rtr_decompose.argtypes = [_vp, ctypes.c_double, P(_i64)]
+    L.rtr_get_csr.argtypes = [_vp, _vp, _vp]
+    L.rtr_get_weights.argtypes = [_vp, _vp, _vp, _vp, P(_i64)]
+    L.rtr_get_status.argtypes = [_vp, _vp]
+    L.rtr_get_clusters.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.rtr_get_cluster_of.argtypes = [_vp, _vp]
+    L.rtr_get_stats.argtypes = [_vp, _vp, P(_i64), P(_i64)]
+    L.rtr_write_decomposition.argtypes = [_vp, ctypes.c_char_p]
+    L.rtr_load_escape.argtypes = [ctypes.c_char_p, P(_i64), P(_i64), P(_vp), P(_vp)]
+    L.rtr_free.argtypes = [_vp]
+    L.rtr_free.restype = None
+    L.rtr_run_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p,
+                               ctypes.c_int]
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = lib().rtr_last_error()
+        raise RtrError(rc, msg.decode() if msg else "")
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class Clusters:
+    """Clusters in creation order (the reference's vector<Cluster>)."""
+    seed: np.ndarray
+    nv: np.ndarray
+    ne: np.ndarray
+    cut: np.ndarray
+    off: np.ndarray
+    vert: np.ndarray
+
+    def __len__(self):
+        return int(self.seed.size)
+
+    def members(self, k: int) -> np.ndarray:
+        return self.vert[self.off[k]:self.off[k + 1]]
+
+
+class Graph:
+    """One graph resident in HBM; stages run on the graph's own CUDA stream."""
+
+    def __init__(self, handle: int):
+        self._h = ctypes.c_void_p(handle)
+
+    # -- construction -------------------------------------------------
+    @classmethod
+    def from_edges(cls, n: int, src, dst, device: int = 0, simplify: bool = False) -> "Graph":
+        src = np.ascontiguousarray(src, dtype=np.int64)
+        dst = np.ascontiguousarray(dst, dtype=np.int64)
+        if src.shape != dst.shape:
+            raise ValueError("src and dst differ in length")
+        h = ctypes.c_void_p()
+        _check(lib().rtr_graph_create_from_edges(_ptr(src), _ptr(dst), src.size, int(n), int(device),
+                                                 RTR_FLAG_SIMPLIFY if simplify else 0, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_csr(cls, offsets, nbors, device: int = 0) -> "Graph":
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        nbors = np.ascontiguousarray(nbors, dtype=np.int64)
+        h = ctypes.c_void_p()
+        _check(lib().rtr_graph_create_from_csr(_ptr(offsets), _ptr(nbors), offsets.size - 1, int(device),
+                                               ctypes.byref(h)))
+        return cls(h.value)
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().rtr_graph_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- info ------------------------------------------------------------
+    @property
+    def n(self) -> int:
+        a, b = _i64(), _i64()
+        _check(lib().rtr_graph_info(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value)
+
+    @property
+    def m(self) -> int:
+        a, b = _i64(), _i64()
+        _check(lib().rtr_graph_info(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return int(b.value)
+
+    # -- stages ----------------------------------------------------------
+    def count(self) -> int:
+        t = _i64()
+        _check(lib().rtr_count(self._h, ctypes.byref(t)))
+        return int(t.value)
+
+    def clean(self, eps: float) -> int:
+        t = _i64()
+        _check(lib().rtr_clean(self._h, float(eps), ctypes.byref(t)))
+        return int(t.value)
+
+    def extract(self) -> int:
+        t = _i64()
+        _check(lib().rtr_extract(self._h, ctypes.byref(t)))
+        return int(t.value)
+
+    def decompose(self, eps: float) -> int:
+        t = _i64()
+        _check(lib().rtr_decompose(self._h, float(eps), ctypes.byref(t)))
+        return int(t.value)
+
+    # -- results -----------------------------------------------------------
+    def csr(self):
+        n, m = self.n, self.m
+        off = np.zeros(n + 1, np.int64)
+        nb = np.zeros(max(1, 2 * m), np.int64)
+        _check(lib().rtr_get_csr(self._h, _ptr(off), _ptr(nb)))
+        return off, nb[:2 * m]
+
+    def weights(self):
+        """(perEdge[2m], perVertex[n], support[2m], total)."""
+        n, m = self.n, self.m
+        pe = np.zeros(max(1, 2 * m), np.float64)
+        pv = np.zeros(max(1, n), np.float64)
+        sup = np.zeros(max(1, 2 * m), np.uint32)
+        t = _i64()
+        _check(lib().rtr_get_weights(self._h, _ptr(pe), _ptr(pv), _ptr(sup), ctypes.byref(t)))
+        return pe[:2 * m], pv[:n], sup[:2 * m], int(t.value)
+
+    def status(self) -> np.ndarray:
+        m = self.m
+        st = np.zeros(max(1, 2 * m), np.uint8)
+        _check(lib().rtr_get_status(self._h, _ptr(st)))
+        return st[:2 * m]
+
+    def clusters(self) -> Clusters:
+        n = self.n
+        cof = self.cluster_of()
+        k = int(cof.max()) + 1 if n else 0
+        seed, nv, ne, cut = (np.zeros(max(1, k), np.int64) for _ in range(4))
+        off = np.zeros(k + 1, np.int64)
+        vert = np.zeros(max(1, n), np.int64)
+        _check(lib().rtr_get_clusters(self._h, _ptr(seed), _ptr(nv), _ptr(ne), _ptr(cut), _ptr(off), _ptr(vert)))
+        return Clusters(seed[:k], nv[:k], ne[:k], cut[:k], off, vert[:n])
+
+    def cluster_of(self) -> np.ndarray:
+        out = np.zeros(max(1, self.n), np.int64)
+        _check(lib().rtr_get_cluster_of(self._h, _ptr(out)))
+        return out[:self.n]
+
+    def stats(self) -> dict:
+        ms = np.zeros(4, np.float64)
+        launches, resid = _i64(), _i64()
+        _check(lib().rtr_get_stats(self._h, _ptr(ms), ctypes.byref(launches), ctypes.byref(resid)))
+        return {"ms_build": ms[0], "ms_count": ms[1], "ms_clean": ms[2], "ms_extract": ms[3],
+                "launches": int(launches.value), "residual_warnings": int(resid.value)}
+
+    def write_decomposition(self, name: str):
+        _check(lib().rtr_write_decomposition(self._h, name.encode()))
+
+
+def load_escape(path: str):
+    """Parse an Escape edge list with the library's loader: (n, src, dst)."""
+    n, m = _i64(), _i64()
+    ps, pd = ctypes.c_void_p(), ctypes.c_void_p()
+    _check(lib().rtr_load_escape(path.encode(), ctypes.byref(n), ctypes.byref(m), ctypes.byref(ps), ctypes.byref(pd)))
+    try:
+        k = int(m.value)
+        src = np.ctypeslib.as_array(ctypes.cast(ps, ctypes.POINTER(ctypes.c_int64)), shape=(max(1, k),))[:k].copy()
+        dst = np.ctypeslib.as_array(ctypes.cast(pd, ctypes.POINTER(ctypes.c_int64)), shape=(max(1, k),))[:k].copy()
+    finally:
+        lib().rtr_free(ps)
+        lib().rtr_free(pd)
+    return int(n.value), src, dst
+
+
+def run_file(path: str, name: str, eps: float, device: int = 0, prefix: str = "RTRex-CUDA-", simplify=False):
+    _check(lib().rtr_run_file(path.encode(), name.encode(), float(eps), int(device), prefix.encode(),
+                              RTR_FLAG_SIMPLIFY if simplify else 0))

@@ -1,0 +1,377 @@
+// C ABI of librtr.so (declared in include/rtr.h).
+#include "../../include/rtr.h"
+#include "primitives.cuh"
+#include "rtr_graph.cuh"
+
+#include <cstdio>
+#include <cstdlib>
+#include <new>
+#include <vector>
+
+namespace rtr {
+const char* last_error();
+}
+
+using namespace rtr;
+
+namespace {
+
+__global__ void k_expand_pe(const double* __restrict__ pe, const uint32_t* __restrict__ sup,
+                            const uint8_t* __restrict__ st, const int32_t* __restrict__ esrc,
+                            const int32_t* __restrict__ nb, const int32_t* __restrict__ partner, int64_t m2,
+                            double* __restrict__ ope, uint32_t* __restrict__ osup, uint8_t* __restrict__ ost)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m2; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t f = (esrc[i] < nb[i]) ? i : (int64_t)partner[i];
+        if (ope) ope[i] = pe[f];
+        if (osup) osup[i] = sup[f];
+        if (ost) ost[i] = st[f];
+    }
+}
+
+__global__ void k_widen32(const int32_t* __restrict__ in, int64_t* __restrict__ out, int64_t k)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
+int make_graph(int64_t n, int device, rtr_graph** out)
+{
+    if (!out) {
+        set_error("null output pointer");
+        return RTR_ERR_ARG;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        set_error("no CUDA device is visible (librtr has no CPU path)");
+        return RTR_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) {
+        set_error("device %d out of range (%d devices)", device, ndev);
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(device));
+    rtr_graph* g = new (std::nothrow) rtr_graph();
+    if (!g) {
+        set_error("host allocation failed");
+        return RTR_ERR_ARG;
+    }
+    g->device = device;
+    g->n = n;
+    if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete g;
+        set_error("cudaStreamCreate failed");
+        return RTR_ERR_CUDA;
+    }
+    g->own_stream = true;
+    g->ctr = (unsigned long long*)dev_alloc(g, 8 * sizeof(unsigned long long));
+    if (!g->ctr) {
+        rtr_graph_destroy(g);
+        set_error("device allocation failed");
+        return RTR_ERR_CUDA;
+    }
+    *out = g;
+    return RTR_OK;
+}
+
+// Typed D2H copy of the first k device int32 values widened to int64.
+int copy_i32_as_i64(rtr_graph* g, const int32_t* d, int64_t k, int64_t* h)
+{
+    if (k <= 0) return RTR_OK;
+    Scratch sc(g);
+    int64_t* w = (int64_t*)sc.get(sizeof(int64_t) * k);
+    if (!w) {
+        set_error("device allocation failed");
+        return RTR_ERR_CUDA;
+    }
+    k_widen32<<<grid_for(k, 256), 256, 0, g->stream>>>(d, w, k);
+    RTR_CUDA_TRY(cudaMemcpyAsync(h, w, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, g->stream));
+    RTR_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    return RTR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rtr_version(void) { return "rtrex-b200 0.1 (sm_100a)"; }
+
+const char* rtr_last_error(void) { return last_error(); }
+
+int rtr_graph_create_from_edges(const int64_t* src, const int64_t* dst, int64_t m, int64_t n, int device, int flags,
+                                rtr_graph** out)
+{
+    if ((!src || !dst) && m > 0) {
+        set_error("null edge arrays");
+        return RTR_ERR_ARG;
+    }
+    int rc = make_graph(n, device, out);
+    if (rc) return rc;
+    rtr_graph* g = *out;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, g->stream);
+    {
+        Scratch sc(g);
+        int64_t* du = (int64_t*)sc.get(sizeof(int64_t) * (m + 1));
+        int64_t* dv = (int64_t*)sc.get(sizeof(int64_t) * (m + 1));
+        if (!du || !dv) {
+            set_error("device allocation failed for %lld edges", (long long)m);
+            rc = RTR_ERR_CUDA;
+        } else {
+            if (m > 0) {
+                cudaMemcpyAsync(du, src, sizeof(int64_t) * m, cudaMemcpyHostToDevice, g->stream);
+                cudaMemcpyAsync(dv, dst, sizeof(int64_t) * m, cudaMemcpyHostToDevice, g->stream);
+            }
+            rc = build_csr(g, du, dv, m, (flags & RTR_FLAG_SIMPLIFY) != 0);
+        }
+    }
+    cudaEventRecord(e1, g->stream);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&g->ms_build, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) {
+        rtr_graph_destroy(g);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int rtr_graph_create_from_csr(const int64_t* offsets, const int64_t* nbors, int64_t n, int device, rtr_graph** out)
+{
+    if (!offsets || (!nbors && offsets[n] > 0)) {
+        set_error("null CSR arrays");
+        return RTR_ERR_ARG;
+    }
+    if (offsets[0] != 0) {
+        set_error("offsets[0] must be 0");
+        return RTR_ERR_INPUT;
+    }
+    for (int64_t v = 0; v < n; ++v)
+        if (offsets[v + 1] < offsets[v]) {
+            set_error("offsets must be non-decreasing (vertex %lld)", (long long)v);
+            return RTR_ERR_INPUT;
+        }
+    int rc = make_graph(n, device, out);
+    if (rc) return rc;
+    rtr_graph* g = *out;
+    rc = build_csr_from_host_csr(g, offsets, nbors);
+    if (rc) {
+        rtr_graph_destroy(g);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int rtr_graph_destroy(rtr_graph* g)
+{
+    if (!g) return RTR_OK;
+    cudaSetDevice(g->device);
+    dev_free_all(g);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return RTR_OK;
+}
+
+int rtr_graph_info(const rtr_graph* g, int64_t* n, int64_t* m)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    if (n) *n = g->n;
+    if (m) *m = g->m;
+    return RTR_OK;
+}
+
+int rtr_count(rtr_graph* g, int64_t* total)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    int rc = count_triangles(g);
+    if (rc) return rc;
+    if (total) {
+        unsigned long long t = 0;
+        RTR_CUDA_TRY(cudaMemcpy(&t, g->ctr, sizeof t, cudaMemcpyDeviceToHost));
+        *total = (int64_t)t;
+    }
+    return RTR_OK;
+}
+
+int rtr_clean(rtr_graph* g, double eps, int64_t* left)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    int rc = initial_clean(g, eps);
+    if (rc) return rc;
+    if (left) {
+        unsigned long long t = 0;
+        RTR_CUDA_TRY(cudaMemcpy(&t, g->ctr, sizeof t, cudaMemcpyDeviceToHost));
+        *left = (int64_t)t;
+    }
+    return RTR_OK;
+}
+
+int rtr_extract(rtr_graph* g, int64_t* ncl)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    int rc = extract_clusters(g);
+    if (rc) return rc;
+    if (ncl) *ncl = g->ncl;
+    return RTR_OK;
+}
+
+int rtr_decompose(rtr_graph* g, double eps, int64_t* ncl)
+{
+    int rc = rtr_count(g, nullptr);
+    if (!rc) rc = rtr_clean(g, eps, nullptr);
+    if (!rc) rc = rtr_extract(g, ncl);
+    return rc;
+}
+
+int rtr_get_csr(const rtr_graph* gc, int64_t* offsets, int64_t* nbors)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || g->stage < 1) {
+        set_error("graph not built");
+        return RTR_ERR_STATE;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    if (offsets) {
+        RTR_CUDA_TRY(cudaMemcpyAsync(offsets, g->offsets, sizeof(int64_t) * (g->n + 1), cudaMemcpyDeviceToHost,
+                                     g->stream));
+        RTR_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    if (nbors) return copy_i32_as_i64(g, g->nbors, g->m2, nbors);
+    return RTR_OK;
+}
+
+int rtr_get_weights(const rtr_graph* gc, double* perEdge, double* perVertex, uint32_t* support, int64_t* total)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || g->stage < 2) {
+        set_error("weights are not computed yet");
+        return RTR_ERR_STATE;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    const int64_t m2 = g->m2;
+    Scratch sc(g);
+    double* ope = perEdge ? (double*)sc.get(sizeof(double) * (m2 + 1)) : nullptr;
+    uint32_t* osup = support ? (uint32_t*)sc.get(sizeof(uint32_t) * (m2 + 1)) : nullptr;
+    if ((perEdge && !ope) || (support && !osup)) {
+        set_error("device allocation failed");
+        return RTR_ERR_CUDA;
+    }
+    if (perEdge || support) {
+        k_expand_pe<<<grid_for(m2, 256), 256, 0, s>>>(g->pe, g->sup, g->st, g->esrc, g->nbors, g->partner, m2, ope,
+                                                       osup, nullptr);
+        RTR_CUDA_TRY(cudaGetLastError());
+    }
+    if (perEdge) RTR_CUDA_TRY(cudaMemcpyAsync(perEdge, ope, sizeof(double) * m2, cudaMemcpyDeviceToHost, s));
+    if (support) RTR_CUDA_TRY(cudaMemcpyAsync(support, osup, sizeof(uint32_t) * m2, cudaMemcpyDeviceToHost, s));
+    if (perVertex) RTR_CUDA_TRY(cudaMemcpyAsync(perVertex, g->pv, sizeof(double) * g->n, cudaMemcpyDeviceToHost, s));
+    if (total) {
+        unsigned long long t = 0;
+        RTR_CUDA_TRY(cudaMemcpyAsync(&t, g->ctr, sizeof t, cudaMemcpyDeviceToHost, s));
+        RTR_CUDA_TRY(cudaStreamSynchronize(s));
+        *total = (int64_t)t;
+    }
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    return RTR_OK;
+}
+
+int rtr_get_status(const rtr_graph* gc, uint8_t* status)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || g->stage < 3 || !status) {
+        set_error("status is not available before the clean");
+        return RTR_ERR_STATE;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    Scratch sc(g);
+    uint8_t* ost = (uint8_t*)sc.get(g->m2 + 16);
+    if (!ost) {
+        set_error("device allocation failed");
+        return RTR_ERR_CUDA;
+    }
+    k_expand_pe<<<grid_for(g->m2, 256), 256, 0, s>>>(g->pe, g->sup, g->st, g->esrc, g->nbors, g->partner, g->m2,
+                                                      nullptr, nullptr, ost);
+    RTR_CUDA_TRY(cudaGetLastError());
+    RTR_CUDA_TRY(cudaMemcpyAsync(status, ost, g->m2, cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    return RTR_OK;
+}
+
+int rtr_get_clusters(const rtr_graph* gc, int64_t* seed, int64_t* nv, int64_t* ne, int64_t* cut, int64_t* off,
+                     int64_t* vert)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || g->stage < 4) {
+        set_error("clusters are not extracted yet");
+        return RTR_ERR_STATE;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    const int64_t k = g->ncl;
+    int rc = RTR_OK;
+    if (seed && (rc = copy_i32_as_i64(g, g->cl_seed, k, seed))) return rc;
+    if (vert && (rc = copy_i32_as_i64(g, g->cl_vert, g->n, vert))) return rc;
+    std::vector<int64_t> o(k + 1);
+    RTR_CUDA_TRY(cudaMemcpyAsync(o.data(), g->cl_off, sizeof(int64_t) * (k + 1), cudaMemcpyDeviceToHost, s));
+    if (ne) RTR_CUDA_TRY(cudaMemcpyAsync(ne, g->cl_ne, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, s));
+    if (cut) RTR_CUDA_TRY(cudaMemcpyAsync(cut, g->cl_cut, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (off)
+        for (int64_t i = 0; i <= k; ++i) off[i] = o[i];
+    if (nv)
+        for (int64_t i = 0; i < k; ++i) nv[i] = o[i + 1] - o[i];
+    return RTR_OK;
+}
+
+int rtr_get_cluster_of(const rtr_graph* gc, int64_t* cluster_of)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || g->stage < 4 || !cluster_of) {
+        set_error("clusters are not extracted yet");
+        return RTR_ERR_STATE;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    return copy_i32_as_i64(g, g->cluster_of, g->n, cluster_of);
+}
+
+int rtr_get_stats(const rtr_graph* g, double* ms4, int64_t* launches, int64_t* residual)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    if (ms4) {
+        ms4[0] = g->ms_build;
+        ms4[1] = g->ms_count;
+        ms4[2] = g->ms_clean;
+        ms4[3] = g->ms_extract;
+    }
+    if (launches) *launches = g->launches;
+    if (residual) *residual = g->diag_residual;
+    return RTR_OK;
+}
+
+void rtr_free(void* p) { free(p); }
+
+}  // extern "C"

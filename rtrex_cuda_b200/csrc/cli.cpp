@@ -1,0 +1,46 @@
+// rtrex_b200: drop-in command line for the decomposition path.
+//
+//   rtrex_b200 <graph_file> <output_name> <eps> [gpu_device] [--prefix P] [--simplify]
+//
+// Same positional arguments and outputs as RTRex_CUDA (RTRex_CUDA/main.cu:343-391):
+// writes <P><output_name>-{decomposition,stats,freq,cut}.txt with P defaulting
+// to "RTRex-CUDA-"; pass --prefix RTRex- for the sequential RTRex driver's names
+// (RTRex_Sequential/clustering/RTRex.cpp:194).  Exit code 1 on any failure,
+// as the reference exits 1 when the graph cannot be loaded.
+#include "../../include/rtr.h"
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+int main(int argc, char** argv)
+{
+    std::string prefix = "RTRex-CUDA-";
+    int flags = 0;
+    const char* pos[4] = {nullptr, nullptr, nullptr, nullptr};
+    int npos = 0;
+    for (int i = 1; i < argc; ++i) {
+        if (!strcmp(argv[i], "--prefix") && i + 1 < argc) {
+            prefix = argv[++i];
+        } else if (!strcmp(argv[i], "--simplify")) {
+            flags |= RTR_FLAG_SIMPLIFY;
+        } else if (npos < 4) {
+            pos[npos++] = argv[i];
+        }
+    }
+    if (npos < 3) {
+        printf("Usage: %s <graph_file> <output_name> <eps> [gpu_device] [--prefix P] [--simplify]\n", argv[0]);
+        return 1;
+    }
+    const double eps = atof(pos[2]);
+    const int device = npos >= 4 ? atoi(pos[3]) : 0;
+    printf("eps = %f\n", eps);
+    const int rc = rtr_run_file(pos[0], pos[1], eps, device, prefix.c_str(), flags);
+    if (rc != RTR_OK) {
+        fprintf(stderr, "Error: %s\n", rtr_last_error());
+        return 1;
+    }
+    printf("[Main] Done.\n");
+    return 0;
+}

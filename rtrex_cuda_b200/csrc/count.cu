@@ -1,0 +1,231 @@
+// Weighted triangle counting, bit-exact to commonNbr
+// (RTRex_Sequential/Escape/Decomposition.h:42-117).
+//
+// commonNbr finds every triangle once, in lexicographic order of its sorted
+// vertex triple, and adds w = 1/double(du*dv*dw) to six directed-edge cells and
+// three vertex cells.  Because of that discovery order:
+//   perEdge[(x,y)]  = left fold, over common neighbours z of x and y in
+//                     ascending z, of w(x,y,z)
+//   perVertex[x]    = left fold over y in N(x) ascending, then over
+//                     z in N(x) & N(y) with z > y ascending, of w(x,y,z)
+// So each cell is produced by one thread as an ordered fold, with no
+// floating-point atomics (the CUDA port's nine atomicAdd(double) per triangle,
+// gpu_triangle_count.cu:70-88, give run-dependent bits).
+//
+// Kernels:
+//   k_edge_fold    one thread per undirected edge: merge / galloping intersection
+//                  of the two rows -> perEdge fold, live support, triangles with z>v
+//   k_tri_fill     same intersection, writes the edge's triangle list
+//                  {z, fwd(a,z), fwd(b,z), deg z} (used by the clean and for perVertex)
+//   k_vertex_fold  one thread per vertex: perVertex fold from the triangle lists
+#include "primitives.cuh"
+#include "rtr_graph.cuh"
+
+namespace rtr {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+// Visit common neighbours of rows [a0,a1) and [b0,b1) in ascending order:
+// f(z, slot_in_a, slot_in_b).  Skewed pairs gallop the short row into the long.
+template <typename F>
+__device__ __forceinline__ void intersect_rows(const int32_t* __restrict__ nb, int64_t a0, int64_t a1, int64_t b0,
+                                               int64_t b1, F&& f)
+{
+    const int64_t la = a1 - a0, lb = b1 - b0;
+    if (la == 0 || lb == 0) return;
+    if (la * 16 < lb || lb * 16 < la) {
+        const bool a_short = la <= lb;
+        const int64_t s0 = a_short ? a0 : b0, s1 = a_short ? a1 : b1;
+        int64_t lo = a_short ? b0 : a0;
+        const int64_t l1 = a_short ? b1 : a1;
+        for (int64_t p = s0; p < s1 && lo < l1; ++p) {
+            const int32_t x = nb[p];
+            int64_t hi = l1;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (nb[mid] < x) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < l1 && nb[lo] == x) {
+                if (a_short) f(x, p, lo);
+                else f(x, lo, p);
+                ++lo;
+            }
+        }
+        return;
+    }
+    int64_t i = a0, j = b0;
+    int32_t x = nb[i], y = nb[j];
+    while (true) {
+        if (x < y) {
+            if (++i >= a1) break;
+            x = nb[i];
+        } else if (x > y) {
+            if (++j >= b1) break;
+            y = nb[j];
+        } else {
+            f(x, i, j);
+            if (++i >= a1 || ++j >= b1) break;
+            x = nb[i];
+            y = nb[j];
+        }
+    }
+}
+
+__device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long* dst)
+{
+    __shared__ unsigned long long s[kBlock / 32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) s[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int k = 0; k < kBlock / 32; ++k) t += s[k];
+        if (t) atomicAdd(dst, t);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_edge_fold(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
+                const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd, int64_t m, double* __restrict__ pe,
+                uint32_t* __restrict__ sup, int64_t* __restrict__ cnt, unsigned long long* __restrict__ total)
+{
+    unsigned long long tri = 0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = fwd[k];
+        const int32_t u = esrc[i], v = nb[i];
+        const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
+        double acc = 0.0;
+        uint32_t c = 0, above = 0;
+        intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], [&](int32_t z, int64_t, int64_t) {
+            acc += 1.0 / (double)(duv * (int64_t)deg[z]);
+            ++c;
+            above += (z > v) ? 1u : 0u;
+        });
+        pe[i] = acc;
+        sup[i] = c;
+        cnt[i] = c;
+        tri += above;
+    }
+    block_add_u64(tri, total);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_tri_fill(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
+               const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, const int32_t* __restrict__ fwd,
+               int64_t m, const int64_t* __restrict__ tl_off, TriEntry* __restrict__ tl)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = fwd[k];
+        const int32_t u = esrc[i], v = nb[i];
+        int64_t w = tl_off[i];
+        intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], [&](int32_t z, int64_t pu, int64_t pv) {
+            TriEntry t;
+            t.z = z;
+            t.eaz = (u < z) ? (int32_t)pu : partner[pu];
+            t.ebz = (v < z) ? (int32_t)pv : partner[pv];
+            t.dz = deg[z];
+            tl[w++] = t;
+        });
+    }
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_vertex_fold(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ deg,
+                  const int32_t* __restrict__ partner, int64_t n, const int64_t* __restrict__ tl_off,
+                  const TriEntry* __restrict__ tl, double* __restrict__ pv)
+{
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t dx = deg[x];
+        double acc = 0.0;
+        for (int64_t i = off[x]; i < off[x + 1]; ++i) {
+            const int32_t y = nb[i];
+            const int64_t c = (x < y) ? i : (int64_t)partner[i];
+            int64_t lo = tl_off[c];
+            const int64_t hi = tl_off[c + 1];
+            if (lo == hi) continue;
+            // first entry with z > y
+            int64_t a = lo, b = hi;
+            while (a < b) {
+                const int64_t mid = (a + b) >> 1;
+                if (tl[mid].z <= y) a = mid + 1;
+                else b = mid;
+            }
+            const int64_t dxy = dx * (int64_t)deg[y];
+            for (int64_t p = a; p < hi; ++p) acc += 1.0 / (double)(dxy * (int64_t)tl[p].dz);
+        }
+        pv[x] = acc;
+    }
+}
+
+}  // namespace
+
+int count_triangles(rtr_graph* g)
+{
+    if (g->stage < 1) {
+        set_error("count called before the graph was built");
+        return RTR_ERR_STATE;
+    }
+    cudaStream_t s = g->stream;
+    const int64_t n = g->n, m2 = g->m2, m = g->m;
+    if (!g->pe) {
+        g->pe = (double*)dev_alloc(g, sizeof(double) * (m2 + 1));
+        g->pv = (double*)dev_alloc(g, sizeof(double) * (n + 1));
+        g->sup = (uint32_t*)dev_alloc(g, sizeof(uint32_t) * (m2 + 1));
+        g->st = (uint8_t*)dev_alloc(g, m2 + 16);
+        g->tl_off = (int64_t*)dev_alloc(g, sizeof(int64_t) * (m2 + 1));
+        if (!g->pe || !g->pv || !g->sup || !g->st || !g->tl_off) {
+            set_error("device allocation failed for the triangle state");
+            return RTR_ERR_CUDA;
+        }
+    }
+    Scratch sc(g);
+    int64_t* cnt = (int64_t*)sc.get(sizeof(int64_t) * (m2 + 1));
+    int64_t* tmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(m2 + 1));
+    if (!cnt || !tmp) {
+        set_error("device allocation failed (count scratch)");
+        return RTR_ERR_CUDA;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    RTR_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, 2 * sizeof(unsigned long long), s));
+    RTR_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int64_t) * (m2 + 1), s));
+    RTR_CUDA_TRY(cudaMemsetAsync(g->pe, 0, sizeof(double) * (m2 + 1), s));
+    RTR_CUDA_TRY(cudaMemsetAsync(g->sup, 0, sizeof(uint32_t) * (m2 + 1), s));
+    const int ge = grid_for(m, kBlock);
+    k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, m, g->pe, g->sup, cnt, g->ctr);
+    exclusive_scan_i64(cnt, g->tl_off, m2 + 1, nullptr, tmp, s);
+    g->launches += 4;
+    RTR_CUDA_TRY(cudaGetLastError());
+    int64_t tl_len = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&tl_len, g->tl_off + m2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (tl_len > g->tl_len || !g->tl) {
+        // grow-only buffer owned by the graph
+        g->tl = (TriEntry*)dev_alloc(g, sizeof(TriEntry) * (tl_len + 1));
+        if (!g->tl) {
+            set_error("device allocation failed for %lld triangle-list entries", (long long)tl_len);
+            return RTR_ERR_CUDA;
+        }
+    }
+    g->tl_len = tl_len;
+    k_tri_fill<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd, m, g->tl_off, g->tl);
+    k_vertex_fold<<<grid_for(n, kBlock), kBlock, 0, s>>>(g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl,
+                                                          g->pv);
+    g->launches += 2;
+    RTR_CUDA_TRY(cudaGetLastError());
+    cudaEventRecord(e1, s);
+    RTR_CUDA_TRY(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(&g->ms_count, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g->stage = 2;
+    return RTR_OK;
+}
+
+}  // namespace rtr

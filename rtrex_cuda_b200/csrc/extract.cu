@@ -1,0 +1,737 @@
+// Cluster extraction, order-faithful to disjointExtract's seed loop
+// (RTRex_Sequential/Escape/Decomposition.h:566-919, populateStats :473-491).
+//
+// Seeds are visited in (degree, id) order (pairCompareSecond, Graph.cpp:40-45).
+// Everything one seed does -- reading alive edges, the two-hop scan, writing
+// triwgt / nbdBitMap / clustered, deleting the cluster's edges and the cascade
+// that follows -- stays inside the seed's connected component of the current
+// alive ('Y') graph, and the alive graph only shrinks.  So the components of
+// the graph left by the initial clean are independent: each is replayed by one
+// thread in the global seed order restricted to it, and performs the
+// reference's floating-point operations in the reference's order.
+//
+// Per-component scratch mirrors the reference's containers:
+//   std::unordered_set members  -> UsetOrder over (key, next, bucket) arrays
+//   std::set two_hop            -> list + ascending sort
+//   std::sort candidates        -> introsort restatement (stl_order.cuh)
+//   std::stack deletion stack   -> array stack
+// Cluster creation order is the global rank of each cluster's seed.
+#include "primitives.cuh"
+#include "rtr_graph.cuh"
+#include "stl_order.cuh"
+
+#include <algorithm>
+
+namespace rtr {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ int64_t fwd_slot(int32_t src, int64_t j, const int32_t* nb, const int32_t* partner)
+{
+    return (src < nb[j]) ? j : (int64_t)partner[j];
+}
+
+__device__ __forceinline__ int64_t find_slot(const int64_t* __restrict__ off, const int32_t* __restrict__ nb,
+                                             int64_t v1, int32_t v2)
+{
+    int64_t lo = off[v1], hi = off[v1 + 1] - 1;
+    while (lo <= hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const int32_t x = nb[mid];
+        if (x == v2) return mid;
+        if (x > v2) hi = mid - 1;
+        else lo = mid + 1;
+    }
+    return -1;
+}
+
+__global__ void k_iota_key_deg(const int32_t* __restrict__ deg, int64_t n, int B, uint64_t* __restrict__ keys)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        keys[v] = ((uint64_t)deg[v] << B) | (uint64_t)v;
+}
+
+__global__ void k_rank(const uint64_t* __restrict__ sorted, int64_t n, uint64_t mask, int32_t* __restrict__ rank,
+                       int32_t* __restrict__ by_rank)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = (int32_t)(sorted[j] & mask);
+        rank[v] = (int32_t)j;
+        by_rank[j] = v;
+    }
+}
+
+__device__ __forceinline__ int32_t uf_find(int32_t* p, int32_t x)
+{
+    while (true) {
+        const int32_t px = p[x];
+        if (px == x) return x;
+        const int32_t ppx = p[px];
+        if (ppx != px) atomicCAS(&p[x], px, ppx);
+        x = px;
+    }
+}
+
+__global__ void k_uf_init(int32_t* __restrict__ p, int64_t n)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        p[v] = (int32_t)v;
+}
+
+__global__ void k_uf_hook_alive(const int32_t* __restrict__ esrc, const int32_t* __restrict__ nb,
+                                const int32_t* __restrict__ fwd, int64_t m, const uint8_t* __restrict__ st,
+                                int32_t* __restrict__ p)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = fwd[k];
+        if (st[i] != ST_Y) continue;
+        int32_t a = esrc[i], b = nb[i];
+        while (true) {
+            a = uf_find(p, a);
+            b = uf_find(p, b);
+            if (a == b) break;
+            if (a > b) {
+                const int32_t t = a;
+                a = b;
+                b = t;
+            }
+            const int32_t old = atomicCAS(&p[b], b, a);
+            if (old == b) break;
+            b = old;
+        }
+    }
+}
+
+__global__ void k_uf_flatten(int32_t* __restrict__ p, int64_t n)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        p[v] = uf_find(p, (int32_t)v);
+}
+
+__global__ void k_alive_count(const int32_t* __restrict__ esrc, const int32_t* __restrict__ fwd, int64_t m,
+                              const uint8_t* __restrict__ st, const int32_t* __restrict__ root,
+                              uint32_t* __restrict__ acount)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = fwd[k];
+        if (st[i] == ST_Y) atomicAdd(&acount[root[esrc[i]]], 1u);
+    }
+}
+
+__global__ void k_comp_keys(const int32_t* __restrict__ root, const int32_t* __restrict__ rank, int64_t n, int R,
+                            uint64_t* __restrict__ keys)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        keys[v] = ((uint64_t)root[v] << R) | (uint64_t)rank[v];
+}
+
+__global__ void k_comp_heads(const uint64_t* __restrict__ keys, int64_t n, int R, const int32_t* __restrict__ by_rank,
+                             uint32_t* __restrict__ head, int32_t* __restrict__ vlist)
+{
+    const uint64_t mask = (1ull << R) - 1;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        head[j] = (j == 0 || (keys[j] >> R) != (keys[j - 1] >> R)) ? 1u : 0u;
+        vlist[j] = by_rank[keys[j] & mask];
+    }
+}
+
+struct CompDesc {
+    int64_t vbegin;   // into vlist / per-vertex scratch
+    int64_t vcount;
+    int64_t bbase;    // bucket scratch
+    int64_t sbase;    // deletion-stack scratch
+    int64_t scap;
+};
+
+__global__ void k_comp_begin(const uint64_t* __restrict__ keys, int64_t n, int R, const uint32_t* __restrict__ head,
+                             const uint32_t* __restrict__ hpos, CompDesc* __restrict__ comps)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+        if (head[j]) comps[hpos[j]].vbegin = j;
+}
+
+__global__ void k_comp_sizes(CompDesc* __restrict__ comps, int64_t nc, int64_t n, const uint64_t* __restrict__ keys,
+                             int R, const uint32_t* __restrict__ acount, int64_t* __restrict__ bneed,
+                             int64_t* __restrict__ sneed)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = comps[c].vbegin;
+        const int64_t e = (c + 1 < nc) ? comps[c + 1].vbegin : n;
+        comps[c].vcount = e - b;
+        bneed[c] = (e - b > 1) ? uset_buckets_after(e - b) + 1 : 0;
+        sneed[c] = acount[(uint32_t)(keys[b] >> R)];
+    }
+}
+
+__global__ void k_comp_finish(CompDesc* __restrict__ comps, int64_t nc, const int64_t* __restrict__ boff,
+                              const int64_t* __restrict__ soff, const int64_t* __restrict__ sneed,
+                              uint64_t* __restrict__ order_keys)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        comps[c].bbase = boff[c];
+        comps[c].sbase = soff[c];
+        comps[c].scap = sneed[c];
+        // largest components first
+        const int64_t wr = comps[c].vcount + sneed[c];
+        const uint64_t w = (uint64_t)(wr < 0xffffffffll ? wr : 0xffffffffll);
+        order_keys[c] = ((uint64_t)(0xffffffffu - (uint32_t)w) << 32) | (uint64_t)c;
+    }
+}
+
+struct Cand {
+    int32_t vertex;
+    int32_t pad;
+    double wgt;
+};
+
+struct DelEntry {
+    int32_t e, first, second, pad;
+};
+
+struct ExtractArgs {
+    const int64_t* off;
+    const int32_t* nb;
+    const int32_t* esrc;
+    const int32_t* partner;
+    const int32_t* deg;
+    const int64_t* tl_off;
+    const TriEntry* tl;
+    double* pe;
+    double* pv;
+    uint32_t* sup;
+    uint8_t* st;
+    double eps;
+    double inv_n;
+    const int32_t* vlist;
+    uint8_t* clustered;
+    uint8_t* nbd;
+    uint8_t* in2hop;
+    double* triwgt;
+    int32_t* ukey;
+    int32_t* unext;
+    int32_t* ubucket;
+    int32_t* twohop;
+    Cand* cand;
+    DelEntry* dstack;
+    int32_t* hdr_seed;
+    int64_t* hdr_start;
+    int32_t* hdr_size;
+    int32_t* out_vert;
+    int32_t* ncl;
+    unsigned* err;
+    unsigned long long* total;
+    unsigned long long* diag;
+};
+
+// deleteAndClean for one thread (Decomposition.h:147-283).
+__device__ void delete_and_clean_seq(const ExtractArgs& a, DelEntry* stack, int64_t top, int64_t cap)
+{
+    long long removed = 0;
+    while (top > 0) {
+        const DelEntry d = stack[--top];
+        const int32_t e = d.e, u = d.first, v = d.second;
+        const uint32_t s_e = a.sup[e];
+        if (s_e == 0) {
+            if (fabs(a.pe[e]) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
+            a.st[e] = ST_N;
+            continue;
+        }
+        const int64_t du = a.deg[u], dv = a.deg[v];
+        const bool lo_is_u = du < dv;
+        const int32_t lower = lo_is_u ? u : v;
+        const int32_t higher = lo_is_u ? v : u;
+        const int64_t dlow = lo_is_u ? du : dv;
+        const int64_t dhigh = lo_is_u ? dv : du;
+        const bool lower_is_a = lower == a.esrc[e];
+        double acc_e = a.pe[e], acc_u = a.pv[u], acc_v = a.pv[v];
+        const int64_t duv = du * dv;
+        uint32_t rem = 0;
+        for (int64_t p = a.tl_off[e]; p < a.tl_off[e + 1]; ++p) {
+            const TriEntry t = a.tl[p];
+            const int32_t elw = lower_is_a ? t.eaz : t.ebz;
+            const int32_t ehw = lower_is_a ? t.ebz : t.eaz;
+            const uint8_t slw = a.st[elw], shw = a.st[ehw];
+            if (slw == ST_N || shw == ST_N) continue;
+            const double wgt = 1 / (double)(duv * (int64_t)t.dz);
+            acc_e -= wgt;
+            const double x1 = a.pe[elw] - wgt;
+            const double x2 = a.pe[ehw] - wgt;
+            a.pe[elw] = x1;
+            a.pe[ehw] = x2;
+            acc_u -= wgt;
+            acc_v -= wgt;
+            a.pv[t.z] -= wgt;
+            a.sup[elw] -= 1u;
+            a.sup[ehw] -= 1u;
+            ++rem;
+            if (slw != ST_S && x1 < a.eps * (1 / (double)(dlow * (int64_t)t.dz))) {
+                if (top >= cap) {
+                    atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                    return;
+                }
+                stack[top++] = DelEntry{elw, lower, t.z, 0};
+                a.st[elw] = ST_S;
+            }
+            if (shw != ST_S && x2 < a.eps * (1 / (double)(dhigh * (int64_t)t.dz))) {
+                if (top >= cap) {
+                    atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                    return;
+                }
+                stack[top++] = DelEntry{ehw, higher, t.z, 0};
+                a.st[ehw] = ST_S;
+            }
+        }
+        a.pe[e] = acc_e;
+        a.pv[u] = acc_u;
+        a.pv[v] = acc_v;
+        a.sup[e] = s_e - rem;
+        removed += rem;
+        if (fabs(acc_e) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
+        a.st[e] = ST_N;
+    }
+    if (removed) atomicAdd(a.total, (unsigned long long)(-removed));
+}
+
+// Ascending sort of distinct vertex ids (the std::set iteration order).
+__device__ void sort_ids(int32_t* x, int64_t n)
+{
+    if (n < 2) return;
+    // heapsort: O(n log n), no extra memory
+    auto sift = [&](int64_t start, int64_t end) {
+        int64_t root = start;
+        while (2 * root + 1 <= end) {
+            int64_t child = 2 * root + 1;
+            if (child + 1 <= end && x[child] < x[child + 1]) ++child;
+            if (x[root] < x[child]) {
+                const int32_t t = x[root];
+                x[root] = x[child];
+                x[child] = t;
+                root = child;
+            } else {
+                return;
+            }
+        }
+    };
+    for (int64_t s = (n - 2) / 2; s >= 0; --s) sift(s, n - 1);
+    for (int64_t end = n - 1; end > 0; --end) {
+        const int32_t t = x[0];
+        x[0] = x[end];
+        x[end] = t;
+        sift(0, end - 1);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const CompDesc* __restrict__ comps,
+                                                            const uint64_t* __restrict__ order, int64_t nc,
+                                                            unsigned* __restrict__ next_comp)
+{
+    while (true) {
+        const unsigned ci = atomicAdd(next_comp, 1u);
+        if ((int64_t)ci >= nc) return;
+        const int64_t c = (int64_t)(uint32_t)order[ci];
+        const CompDesc cd = comps[c];
+        const int64_t vb = cd.vbegin, nv = cd.vcount;
+        if (nv == 1) {  // an isolated vertex: a singleton cluster with no edges to delete
+            const int32_t u = a.vlist[vb];
+            a.clustered[u] = 1;
+            a.hdr_seed[vb] = u;
+            a.hdr_start[vb] = vb;
+            a.hdr_size[vb] = 1;
+            a.out_vert[vb] = u;
+            a.ncl[c] = 1;
+            continue;
+        }
+        int32_t* ukey = a.ukey + vb;
+        int32_t* unext = a.unext + vb;
+        int32_t* ubucket = a.ubucket + cd.bbase;
+        int32_t* twohop = a.twohop + vb;
+        Cand* cand = a.cand + vb;
+        DelEntry* dstack = a.dstack + cd.sbase;
+        int64_t out = vb;
+        int32_t ncl = 0;
+        for (int64_t idx = 0; idx < nv; ++idx) {
+            const int32_t u = a.vlist[vb + idx];
+            if (a.clustered[u]) continue;
+            const int64_t du = a.deg[u];
+            UsetOrder S;
+            S.init(ukey, unext, ubucket);
+            S.insert(u);
+            a.clustered[u] = 1;
+            const int64_t r0 = a.off[u], r1 = a.off[u + 1];
+            for (int64_t j = r0; j < r1; ++j) {
+                if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
+                const int32_t v = a.nb[j];
+                S.insert(v);
+                a.nbd[v] = 1;
+                a.clustered[v] = 1;
+            }
+            double internal = 0;
+            int64_t n2 = 0;
+            const double thr = (double)du / a.eps;
+            for (int64_t j = r0; j < r1; ++j) {
+                if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
+                const int32_t v = a.nb[j];
+                const int64_t dv = a.deg[v];
+                if ((double)dv > thr) continue;
+                for (int64_t k = j; k < r1; ++k) {  // k starts at j: w == v included
+                    if (a.st[fwd_slot(u, k, a.nb, a.partner)] == ST_N) continue;
+                    const int32_t w = a.nb[k];
+                    const int64_t dw = a.deg[w];
+                    if ((double)dw > thr) continue;
+                    internal += 1.0 / (double)(du * dv * dw);
+                    const int32_t lower = (dv < dw) ? v : w;
+                    const int32_t higher = (dv < dw) ? w : v;
+                    for (int64_t l = a.off[lower]; l < a.off[lower + 1]; ++l) {
+                        if (a.st[fwd_slot(lower, l, a.nb, a.partner)] == ST_N) continue;
+                        const int32_t x = a.nb[l];
+                        if (x == lower || x == higher || x == u) continue;
+                        const int64_t lh = find_slot(a.off, a.nb, higher, x);
+                        if (lh < 0 || a.st[fwd_slot(higher, lh, a.nb, a.partner)] == ST_N) continue;
+                        const double wgt = 1.0 / (double)((int64_t)a.deg[x] * dv * dw);
+                        if (a.nbd[x]) {
+                            if (x > v && x > w) internal += wgt;
+                            continue;
+                        }
+                        if (!a.in2hop[x]) {
+                            a.in2hop[x] = 1;
+                            twohop[n2++] = x;
+                        }
+                        a.triwgt[x] += wgt;
+                    }
+                }
+            }
+            sort_ids(twohop, n2);
+            double potential = 0;
+            for (int64_t k = 0; k < n2; ++k) {
+                const int32_t x = twohop[k];
+                cand[k].vertex = x;
+                cand[k].pad = 0;
+                cand[k].wgt = a.triwgt[x];
+                potential += a.triwgt[x];
+                a.triwgt[x] = 0;
+                a.in2hop[x] = 0;
+            }
+            introsort(cand, cand + n2, [](const Cand& p, const Cand& q) { return p.wgt > q.wgt; });
+            double ratio = internal / (internal + potential);
+            int64_t maxind = -1;
+            double num = 0, den = 0;
+            for (int64_t k = 0; k < n2; ++k) {
+                num += cand[k].wgt;
+                den += a.pv[cand[k].vertex];
+                const double nr = (internal + num) / (internal + potential + den);
+                if (nr > ratio) {
+                    ratio = nr;
+                    maxind = k;
+                }
+            }
+            for (int64_t k = 0; k <= maxind; ++k) {
+                S.insert(cand[k].vertex);
+                a.clustered[cand[k].vertex] = 1;
+            }
+            for (int64_t j = r0; j < r1; ++j) a.nbd[a.nb[j]] = 0;
+
+            if (out + S.size > vb + nv || ncl >= nv) {  // clusters must partition the component
+                atomicOr(a.err, (unsigned)DEV_ERR_SCRATCH);
+                break;
+            }
+            a.hdr_seed[vb + ncl] = u;
+            a.hdr_start[vb + ncl] = out;
+            a.hdr_size[vb + ncl] = S.size;
+            for (int32_t p = S.head; p != -1; p = S.next[p]) a.out_vert[out++] = S.key[p];
+            ++ncl;
+
+            int64_t top = 0;
+            for (int32_t p = S.head; p != -1; p = S.next[p]) {
+                const int32_t z = S.key[p];
+                for (int64_t j = a.off[z]; j < a.off[z + 1]; ++j) {
+                    const int64_t f = fwd_slot(z, j, a.nb, a.partner);
+                    if (a.st[f] != ST_Y) continue;
+                    if (top >= cd.scap) {
+                        atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                        break;
+                    }
+                    dstack[top++] = DelEntry{(int32_t)f, z, a.nb[j], 0};
+                    a.st[f] = ST_S;
+                }
+            }
+            delete_and_clean_seq(a, dstack, top, cd.scap);
+        }
+        a.ncl[c] = ncl;
+    }
+}
+
+__global__ void k_cluster_keys(const CompDesc* __restrict__ comps, int64_t nc, const int32_t* __restrict__ ncl,
+                               const int64_t* __restrict__ cpos, const int32_t* __restrict__ hdr_seed,
+                               const int32_t* __restrict__ rank, int B, uint64_t* __restrict__ keys)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t vb = comps[c].vbegin;
+        for (int32_t k = 0; k < ncl[c]; ++k)
+            keys[cpos[c] + k] = ((uint64_t)rank[hdr_seed[vb + k]] << B) | (uint64_t)(vb + k);
+    }
+}
+
+__global__ void k_cluster_gather(const uint64_t* __restrict__ sorted, int64_t ncl, uint64_t mask,
+                                 const int32_t* __restrict__ hdr_seed, const int32_t* __restrict__ hdr_size,
+                                 int32_t* __restrict__ cl_seed, int64_t* __restrict__ size64)
+{
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ncl; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t h = (int64_t)(sorted[g] & mask);
+        cl_seed[g] = hdr_seed[h];
+        size64[g] = hdr_size[h];
+    }
+}
+
+__global__ void k_cluster_members(const uint64_t* __restrict__ sorted, int64_t ncl, uint64_t mask,
+                                  const int64_t* __restrict__ hdr_start, const int64_t* __restrict__ cl_off,
+                                  const int32_t* __restrict__ out_vert, int32_t* __restrict__ cl_vert,
+                                  int32_t* __restrict__ cluster_of)
+{
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ncl; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t h = (int64_t)(sorted[g] & mask);
+        const int64_t src = hdr_start[h];
+        for (int64_t p = cl_off[g]; p < cl_off[g + 1]; ++p) {
+            const int32_t v = out_vert[src + (p - cl_off[g])];
+            cl_vert[p] = v;
+            cluster_of[v] = (int32_t)g;
+        }
+    }
+}
+
+// populateStats over the original adjacency (integer counts, order-free).
+__global__ void k_cluster_stats(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, int64_t n,
+                                const int32_t* __restrict__ cluster_of, unsigned long long* __restrict__ ne,
+                                unsigned long long* __restrict__ cut)
+{
+    for (int64_t z = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; z < n; z += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = cluster_of[z];
+        unsigned long long in = 0, outc = 0;
+        for (int64_t j = off[z]; j < off[z + 1]; ++j) {
+            if (cluster_of[nb[j]] == c) ++in;
+            else ++outc;
+        }
+        if (in) atomicAdd(&ne[c], in);
+        if (outc) atomicAdd(&cut[c], outc);
+    }
+}
+
+__global__ void k_widen(const int32_t* __restrict__ in, int64_t* __restrict__ out, int64_t k)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
+__global__ void k_halve(int64_t* __restrict__ ne, int64_t ncl)
+{
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ncl; g += (int64_t)gridDim.x * blockDim.x)
+        ne[g] /= 2;
+}
+
+}  // namespace
+
+int extract_clusters(rtr_graph* g)
+{
+    if (g->stage < 3) {
+        set_error("extract called before the clean");
+        return RTR_ERR_STATE;
+    }
+    cudaStream_t s = g->stream;
+    const int64_t n = g->n, m = g->m, m2 = g->m2;
+    Scratch sc(g);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    RTR_CUDA_TRY(cudaMemsetAsync(g->ctr + 1, 0, 2 * sizeof(unsigned long long), s));
+
+    const int B = bits_for((uint64_t)(n - 1));
+    const uint64_t bmask = (1ull << B) - 1;
+    const int gn = grid_for(n, kBlock), gm = grid_for(m, kBlock);
+
+    // global seed order: (degree, id)
+    uint64_t* k1 = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
+    uint64_t* k2 = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
+    void* rtmp = sc.get(radix_temp_bytes(n));
+    int32_t* rank = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    int32_t* by_rank = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    int32_t* root = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    uint32_t* acount = (uint32_t*)sc.get(sizeof(uint32_t) * (n + 1));
+    uint32_t* head = (uint32_t*)sc.get(sizeof(uint32_t) * (n + 1));
+    uint32_t* hpos = (uint32_t*)sc.get(sizeof(uint32_t) * (n + 1));
+    uint32_t* htmp = (uint32_t*)sc.get(sizeof(uint32_t) * scan_temp_elems(n + 1));
+    uint32_t* d_nc = (uint32_t*)sc.get(sizeof(uint32_t) * 2);
+    int32_t* vlist = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    if (!k1 || !k2 || !rtmp || !rank || !by_rank || !root || !acount || !head || !hpos || !htmp || !d_nc || !vlist) {
+        set_error("device allocation failed (extract setup)");
+        return RTR_ERR_CUDA;
+    }
+    k_iota_key_deg<<<gn, kBlock, 0, s>>>(g->deg, n, B, k1);
+    uint64_t* sorted = radix_sort_u64(k1, k2, n, B + bits_for((uint64_t)m2), rtmp, s);
+    k_rank<<<gn, kBlock, 0, s>>>(sorted, n, bmask, rank, by_rank);
+    // components of the alive graph
+    k_uf_init<<<gn, kBlock, 0, s>>>(root, n);
+    k_uf_hook_alive<<<gm, kBlock, 0, s>>>(g->esrc, g->nbors, g->fwd, m, g->st, root);
+    k_uf_flatten<<<gn, kBlock, 0, s>>>(root, n);
+    RTR_CUDA_TRY(cudaMemsetAsync(acount, 0, sizeof(uint32_t) * (n + 1), s));
+    k_alive_count<<<gm, kBlock, 0, s>>>(g->esrc, g->fwd, m, g->st, root, acount);
+    k_comp_keys<<<gn, kBlock, 0, s>>>(root, rank, n, B, k1 == sorted ? k2 : k1);
+    uint64_t* ck = (k1 == sorted) ? k2 : k1;
+    uint64_t* calt = sorted;  // rank/by_rank already captured; reuse as ping-pong
+    uint64_t* csorted = radix_sort_u64(ck, calt, n, 2 * B, rtmp, s);
+    k_comp_heads<<<gn, kBlock, 0, s>>>(csorted, n, B, by_rank, head, vlist);
+    exclusive_scan_u32(head, hpos, n, d_nc, htmp, s);
+    g->launches += 12 + 3 * ((B + bits_for((uint64_t)m2) + 7) / 8) + 3 * ((2 * B + 7) / 8);
+    RTR_CUDA_TRY(cudaGetLastError());
+    uint32_t nc = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&nc, d_nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+
+    CompDesc* comps = (CompDesc*)sc.get(sizeof(CompDesc) * (nc + 1));
+    int64_t* bneed = (int64_t*)sc.get(sizeof(int64_t) * (nc + 1));
+    int64_t* sneed = (int64_t*)sc.get(sizeof(int64_t) * (nc + 1));
+    int64_t* boff = (int64_t*)sc.get(sizeof(int64_t) * (nc + 1));
+    int64_t* soff = (int64_t*)sc.get(sizeof(int64_t) * (nc + 1));
+    int64_t* ltmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(nc + 1));
+    int64_t* d_tot = (int64_t*)sc.get(sizeof(int64_t) * 2);
+    uint64_t* okeys = (uint64_t*)sc.get(sizeof(uint64_t) * (nc + 1));
+    uint64_t* oalt = (uint64_t*)sc.get(sizeof(uint64_t) * (nc + 1));
+    void* otmp = sc.get(radix_temp_bytes(nc));
+    if (!comps || !bneed || !sneed || !boff || !soff || !ltmp || !d_tot || !okeys || !oalt || !otmp) {
+        set_error("device allocation failed (extract components)");
+        return RTR_ERR_CUDA;
+    }
+    k_comp_begin<<<gn, kBlock, 0, s>>>(csorted, n, B, head, hpos, comps);
+    const int gc = grid_for(nc, kBlock);
+    k_comp_sizes<<<gc, kBlock, 0, s>>>(comps, nc, n, csorted, B, acount, bneed, sneed);
+    exclusive_scan_i64(bneed, boff, nc, d_tot, ltmp, s);
+    exclusive_scan_i64(sneed, soff, nc, d_tot + 1, ltmp, s);
+    k_comp_finish<<<gc, kBlock, 0, s>>>(comps, nc, boff, soff, sneed, okeys);
+    uint64_t* order = radix_sort_u64(okeys, oalt, nc, 64, otmp, s);
+    g->launches += 9 + 24;
+    int64_t tots[2] = {0, 0};
+    RTR_CUDA_TRY(cudaMemcpyAsync(tots, d_tot, sizeof tots, cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+
+    ExtractArgs a;
+    a.off = g->offsets;
+    a.nb = g->nbors;
+    a.esrc = g->esrc;
+    a.partner = g->partner;
+    a.deg = g->deg;
+    a.tl_off = g->tl_off;
+    a.tl = g->tl;
+    a.pe = g->pe;
+    a.pv = g->pv;
+    a.sup = g->sup;
+    a.st = g->st;
+    a.eps = g->eps;
+    a.inv_n = 1 / (double)n;
+    a.vlist = vlist;
+    a.clustered = (uint8_t*)sc.get(n + 16);
+    a.nbd = (uint8_t*)sc.get(n + 16);
+    a.in2hop = (uint8_t*)sc.get(n + 16);
+    a.triwgt = (double*)sc.get(sizeof(double) * (n + 1));
+    a.ukey = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    a.unext = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    a.ubucket = (int32_t*)sc.get(sizeof(int32_t) * (tots[0] + 1));
+    a.twohop = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    a.cand = (Cand*)sc.get(sizeof(Cand) * (n + 1));
+    a.dstack = (DelEntry*)sc.get(sizeof(DelEntry) * (tots[1] + 1));
+    a.hdr_seed = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    a.hdr_start = (int64_t*)sc.get(sizeof(int64_t) * (n + 1));
+    a.hdr_size = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    a.out_vert = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    a.ncl = (int32_t*)sc.get(sizeof(int32_t) * (nc + 1));
+    a.err = (unsigned*)(g->ctr + 1);
+    a.total = g->ctr;
+    a.diag = g->ctr + 2;
+    unsigned* next_comp = (unsigned*)sc.get(sizeof(unsigned) * 2);
+    if (!a.clustered || !a.nbd || !a.in2hop || !a.triwgt || !a.ukey || !a.unext || !a.ubucket || !a.twohop ||
+        !a.cand || !a.dstack || !a.hdr_seed || !a.hdr_start || !a.hdr_size || !a.out_vert || !a.ncl || !next_comp) {
+        set_error("device allocation failed (extract scratch)");
+        return RTR_ERR_CUDA;
+    }
+    RTR_CUDA_TRY(cudaMemsetAsync(a.clustered, 0, n + 16, s));
+    RTR_CUDA_TRY(cudaMemsetAsync(a.nbd, 0, n + 16, s));
+    RTR_CUDA_TRY(cudaMemsetAsync(a.in2hop, 0, n + 16, s));
+    RTR_CUDA_TRY(cudaMemsetAsync(a.triwgt, 0, sizeof(double) * (n + 1), s));
+    RTR_CUDA_TRY(cudaMemsetAsync(next_comp, 0, sizeof(unsigned) * 2, s));
+    {
+        const int blk = 128;
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nc + blk - 1) / blk, grid_for(1 << 30, blk, 16)));
+        k_extract_components<<<blocks, blk, 0, s>>>(a, comps, order, nc, next_comp);
+        g->launches += 1;
+    }
+    RTR_CUDA_TRY(cudaGetLastError());
+
+    // clusters in creation order = ascending rank of their seeds
+    int64_t* cpos = (int64_t*)sc.get(sizeof(int64_t) * (nc + 1));
+    int64_t* ncl64 = (int64_t*)sc.get(sizeof(int64_t) * (nc + 1));
+    if (!cpos || !ncl64) {
+        set_error("device allocation failed (cluster order)");
+        return RTR_ERR_CUDA;
+    }
+    k_widen<<<gc, kBlock, 0, s>>>(a.ncl, ncl64, nc);
+    exclusive_scan_i64(ncl64, cpos, nc, d_tot, ltmp, s);
+    int64_t ncl = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&ncl, d_tot, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    {
+        unsigned long long h[3];
+        RTR_CUDA_TRY(cudaMemcpy(h, g->ctr, sizeof h, cudaMemcpyDeviceToHost));
+        if (h[1] != 0) {
+            set_error("device error word 0x%llx during extraction", h[1]);
+            return RTR_ERR_DEVICE;
+        }
+        g->diag_residual += (long long)h[2];
+    }
+    uint64_t* ckeys = (uint64_t*)sc.get(sizeof(uint64_t) * (ncl + 1));
+    uint64_t* calt2 = (uint64_t*)sc.get(sizeof(uint64_t) * (ncl + 1));
+    void* ctmp = sc.get(radix_temp_bytes(ncl));
+    int64_t* size64 = (int64_t*)sc.get(sizeof(int64_t) * (ncl + 1));
+    if (!ckeys || !calt2 || !ctmp || !size64) {
+        set_error("device allocation failed (cluster keys)");
+        return RTR_ERR_CUDA;
+    }
+    if (!g->cl_seed || g->ncl < ncl) {
+        g->cl_seed = (int32_t*)dev_alloc(g, sizeof(int32_t) * (ncl + 1));
+        g->cl_off = (int64_t*)dev_alloc(g, sizeof(int64_t) * (ncl + 2));
+        g->cl_ne = (int64_t*)dev_alloc(g, sizeof(int64_t) * (ncl + 1));
+        g->cl_cut = (int64_t*)dev_alloc(g, sizeof(int64_t) * (ncl + 1));
+    }
+    if (!g->cl_vert) {
+        g->cl_vert = (int32_t*)dev_alloc(g, sizeof(int32_t) * (n + 1));
+        g->cluster_of = (int32_t*)dev_alloc(g, sizeof(int32_t) * (n + 1));
+    }
+    if (!g->cl_seed || !g->cl_off || !g->cl_ne || !g->cl_cut || !g->cl_vert || !g->cluster_of) {
+        set_error("device allocation failed (cluster outputs)");
+        return RTR_ERR_CUDA;
+    }
+    g->ncl = ncl;
+    RTR_CUDA_TRY(cudaMemsetAsync(size64, 0, sizeof(int64_t) * (ncl + 1), s));
+    k_cluster_keys<<<gc, kBlock, 0, s>>>(comps, nc, a.ncl, cpos, a.hdr_seed, rank, B, ckeys);
+    uint64_t* csort = radix_sort_u64(ckeys, calt2, ncl, 2 * B, ctmp, s);
+    const int gk = grid_for(ncl, kBlock);
+    k_cluster_gather<<<gk, kBlock, 0, s>>>(csort, ncl, bmask, a.hdr_seed, a.hdr_size, g->cl_seed, size64);
+    exclusive_scan_i64(size64, g->cl_off, ncl + 1, nullptr, ltmp, s);
+    k_cluster_members<<<gk, kBlock, 0, s>>>(csort, ncl, bmask, a.hdr_start, g->cl_off, a.out_vert, g->cl_vert,
+                                            g->cluster_of);
+    RTR_CUDA_TRY(cudaMemsetAsync(g->cl_ne, 0, sizeof(int64_t) * (ncl + 1), s));
+    RTR_CUDA_TRY(cudaMemsetAsync(g->cl_cut, 0, sizeof(int64_t) * (ncl + 1), s));
+    k_cluster_stats<<<gn, kBlock, 0, s>>>(g->offsets, g->nbors, n, g->cluster_of,
+                                          (unsigned long long*)g->cl_ne, (unsigned long long*)g->cl_cut);
+    k_halve<<<gk, kBlock, 0, s>>>(g->cl_ne, ncl);
+    g->launches += 8 + 3 * ((2 * B + 7) / 8);
+    RTR_CUDA_TRY(cudaGetLastError());
+    cudaEventRecord(e1, s);
+    RTR_CUDA_TRY(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(&g->ms_extract, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g->stage = 4;
+    return RTR_OK;
+}
+
+}  // namespace rtr

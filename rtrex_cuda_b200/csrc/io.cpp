@@ -1,0 +1,258 @@
+// Host side of the drop-in surface: the Escape edge-list parser, the
+// decomposition writer and the whole-file driver.
+#include "../../include/rtr.h"
+
+#include <algorithm>
+#include <cerrno>
+#include <cinttypes>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace rtr {
+void set_error(const char* fmt, ...);
+}
+
+namespace {
+
+bool blank(const char* p, const char* e)
+{
+    for (; p < e; ++p)
+        if (!(*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n' || *p == '\v' || *p == '\f')) return false;
+    return true;
+}
+
+// strtoll-like: skips leading blanks, optional sign, decimal digits.
+bool parse_i64(const char*& p, const char* e, int64_t* out)
+{
+    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f')) ++p;
+    bool neg = false;
+    if (p < e && (*p == '-' || *p == '+')) {
+        neg = *p == '-';
+        ++p;
+    }
+    if (p >= e || *p < '0' || *p > '9') return false;
+    int64_t v = 0;
+    while (p < e && *p >= '0' && *p <= '9') v = v * 10 + (*p++ - '0');
+    *out = neg ? -v : v;
+    return true;
+}
+
+struct ClusterView {
+    int64_t nv, ne, idx;
+};
+
+}  // namespace
+
+extern "C" {
+
+// loadGraph_Escape (RTRex_Sequential/GraphIO.cpp:19-74): comment lines start
+// with '#', blank lines are skipped, the first data line is "n m", every other
+// data line is one undirected pair.
+int rtr_load_escape(const char* path, int64_t* n_out, int64_t* m_out, int64_t** src_out, int64_t** dst_out)
+{
+    if (!path || !n_out || !m_out || !src_out || !dst_out) {
+        rtr::set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    *src_out = *dst_out = nullptr;
+    FILE* f = fopen(path, "rb");
+    if (!f) {
+        rtr::set_error("could not open file %s", path);
+        return RTR_ERR_IO;
+    }
+    std::vector<char> buf;
+    {
+        fseek(f, 0, SEEK_END);
+        long sz = ftell(f);
+        fseek(f, 0, SEEK_SET);
+        buf.resize(sz > 0 ? (size_t)sz : 0);
+        if (sz > 0 && fread(buf.data(), 1, (size_t)sz, f) != (size_t)sz) {
+            fclose(f);
+            rtr::set_error("short read on %s", path);
+            return RTR_ERR_IO;
+        }
+        fclose(f);
+    }
+    const char* p = buf.data();
+    const char* end = p + buf.size();
+    bool have_header = false;
+    int64_t n = 0, m = 0, got = 0, lineno = 0;
+    int64_t *src = nullptr, *dst = nullptr;
+    while (p < end) {
+        const char* nl = (const char*)memchr(p, '\n', (size_t)(end - p));
+        const char* le = nl ? nl : end;
+        ++lineno;
+        if (*p != '#' && !blank(p, le)) {
+            const char* q = p;
+            int64_t a = 0, b = 0;
+            if (!parse_i64(q, le, &a) || !parse_i64(q, le, &b)) {
+                free(src);
+                free(dst);
+                rtr::set_error("%s:%lld: expected two integers", path, (long long)lineno);
+                return RTR_ERR_IO;
+            }
+            if (!have_header) {
+                have_header = true;
+                n = a;
+                m = b;
+                if (n < 0 || m < 0) {
+                    rtr::set_error("%s: negative header values", path);
+                    return RTR_ERR_IO;
+                }
+                src = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m > 0 ? m : 1));
+                dst = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m > 0 ? m : 1));
+                if (!src || !dst) {
+                    free(src);
+                    free(dst);
+                    rtr::set_error("host allocation failed for %lld edges", (long long)m);
+                    return RTR_ERR_IO;
+                }
+            } else if (got < m) {
+                src[got] = a;
+                dst[got] = b;
+                ++got;
+            }
+        }
+        p = nl ? nl + 1 : end;
+    }
+    if (!have_header) {
+        rtr::set_error("%s: no header line", path);
+        return RTR_ERR_IO;
+    }
+    if (got < m) {
+        free(src);
+        free(dst);
+        // the reference reports edges counted in both directions (GraphIO.cpp:67-71)
+        rtr::set_error("expected %" PRId64 " edges, only got %" PRId64, 2 * m, 2 * got);
+        return RTR_ERR_IO;
+    }
+    *n_out = n;
+    *m_out = m;
+    *src_out = src;
+    *dst_out = dst;
+    return RTR_OK;
+}
+
+// printDecomposition (RTRex_Sequential/clustering/RTRex.cpp:19-118).  Clusters
+// are ranked with std::sort on the size comparator from creation order, as the
+// reference does, so equal-size clusters land in the same lines; members are
+// written in the reference's set-iteration order.
+int rtr_write_decomposition(const rtr_graph* g, const char* name_c)
+{
+    if (!g || !name_c) {
+        rtr::set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    int64_t n = 0, m = 0, k = 0;
+    int rc = rtr_graph_info(g, &n, &m);
+    if (rc) return rc;
+    std::vector<int64_t> off(n + 1), nb(2 * m), cluster_of(n);
+    if ((rc = rtr_get_csr(g, off.data(), nb.data()))) return rc;
+    if ((rc = rtr_get_cluster_of(g, cluster_of.data()))) return rc;
+    for (int64_t v = 0; v < n; ++v) k = std::max(k, cluster_of[v] + 1);
+    std::vector<int64_t> seed(k), nv(k), ne(k), cut(k), coff(k + 1), vert(n);
+    if ((rc = rtr_get_clusters(g, seed.data(), nv.data(), ne.data(), cut.data(), coff.data(), vert.data())))
+        return rc;
+
+    const std::string name(name_c);
+    printf("\n--------------------------------------------\n");
+    printf("Generating details of %s decomposition\n", name.c_str());
+    FILE* f = fopen((name + "-decomposition.txt").c_str(), "w");
+    FILE* fs = fopen((name + "-stats.txt").c_str(), "w");
+    FILE* fcut = fopen((name + "-cut.txt").c_str(), "w");
+    FILE* ffreq = fopen((name + "-freq.txt").c_str(), "w");
+    if (!f || !fs || !fcut || !ffreq) {
+        if (f) fclose(f);
+        if (fs) fclose(fs);
+        if (fcut) fclose(fcut);
+        if (ffreq) fclose(ffreq);
+        rtr::set_error("could not write the output files for %s", name.c_str());
+        return RTR_ERR_IO;
+    }
+    std::vector<ClusterView> cl(k);
+    for (int64_t i = 0; i < k; ++i) cl[i] = ClusterView{nv[i], ne[i], i};
+    std::sort(cl.begin(), cl.end(), [](const ClusterView& a, const ClusterView& b) { return a.nv > b.nv; });
+    std::vector<int64_t> freq(n + 1, 0);
+    int64_t maxsize = 0, total_clustered = 0, total_internal = 0;
+    std::string line;
+    for (int64_t r = 0; r < k; ++r) {
+        const ClusterView& c = cl[r];
+        line.clear();
+        char tmp[32];
+        for (int64_t p = coff[c.idx]; p < coff[c.idx + 1]; ++p) {
+            int len = snprintf(tmp, sizeof tmp, "%" PRId64 " ", vert[p]);
+            line.append(tmp, (size_t)len);
+        }
+        line.push_back('\n');
+        fwrite(line.data(), 1, line.size(), f);
+        if (c.nv > maxsize) maxsize = c.nv;
+        freq[c.nv]++;
+        if (c.nv != 1) {
+            const double density = 2 * (c.ne) / ((double)(c.nv) * (double)(c.nv - 1));
+            total_clustered += c.nv;
+            total_internal += c.ne;
+            fprintf(fs, "%" PRId64 " %.2f\n", c.nv, density);
+        }
+        for (int64_t p = coff[c.idx]; p < coff[c.idx + 1]; ++p) {
+            const int64_t vtx = vert[p];
+            for (int64_t j = off[vtx]; j < off[vtx + 1]; ++j) {
+                const int64_t nbr = nb[j];
+                if (nbr < vtx) continue;
+                if (cluster_of[nbr] != c.idx) fprintf(fcut, "%" PRId64 " %" PRId64 "\n", vtx, nbr);
+            }
+        }
+    }
+    printf("Non-trivial clustered vertices: %" PRId64 "\n", total_clustered);
+    printf("Edges inside clusters: %" PRId64 "\n", total_internal);
+    printf("\n--------------------------------------------\n");
+    for (int64_t i = 0; i < maxsize + 1; ++i)
+        fprintf(ffreq, "Size = %" PRId64 ", freq = %" PRId64 ", total vertices = %" PRId64 "\n", i, freq[i],
+                i * freq[i]);
+    fclose(fs);
+    fclose(ffreq);
+    fclose(fcut);
+    fclose(f);
+    return RTR_OK;
+}
+
+int rtr_run_file(const char* graph_path, const char* name, double eps, int device, const char* prefix, int flags)
+{
+    if (!graph_path || !name) {
+        rtr::set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    int64_t n = 0, m = 0;
+    int64_t *src = nullptr, *dst = nullptr;
+    int rc = rtr_load_escape(graph_path, &n, &m, &src, &dst);
+    if (rc) return rc;
+    printf("Loaded graph\nVertices = %" PRId64 "\nEdges = %" PRId64 "\n", n, m);
+    rtr_graph* g = nullptr;
+    rc = rtr_graph_create_from_edges(src, dst, m, n, device, flags, &g);
+    free(src);
+    free(dst);
+    if (rc) return rc;
+    int64_t total = 0, left = 0, ncl = 0;
+    if (!(rc = rtr_count(g, &total))) {
+        printf("Total triangles = %" PRId64 "\n", total);
+        if (!(rc = rtr_clean(g, eps, &left))) {
+            printf("Total triangle count, post cleaning = %" PRId64 "\n", left);
+            rc = rtr_extract(g, &ncl);
+        }
+    }
+    if (!rc) {
+        double ms[4];
+        rtr_get_stats(g, ms, nullptr, nullptr);
+        printf("Time for getting the weights: %gs \n", ms[1] / 1e3);
+        printf("Time for the initial clean: %gs \n", ms[2] / 1e3);
+        printf("Time for getting the clusters: %gs \n", ms[3] / 1e3);
+        printf("Total clusters extracted: %" PRId64 "\n", ncl);
+        rc = rtr_write_decomposition(g, (std::string(prefix ? prefix : "") + name).c_str());
+    }
+    rtr_graph_destroy(g);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// Host-side handle for one graph resident in HBM, and the stage entry points
+// the C ABI (capi.cu) drives.  All device work of a graph runs on its own
+// stream; calls on different graphs may run concurrently.
+#pragma once
+
+#include "rtr_common.cuh"
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+struct rtr_graph {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    int64_t n = 0;   // vertices
+    int64_t m2 = 0;  // directed slots (2 x undirected edges)
+    int64_t m = 0;   // undirected edges
+
+    // CSR (see rtr_common.cuh for the layout)
+    int64_t* offsets = nullptr;
+    int32_t* nbors = nullptr;
+    int32_t* esrc = nullptr;
+    int32_t* partner = nullptr;
+    int32_t* deg = nullptr;
+    int32_t* fwd = nullptr;  // the m forward slots, ascending
+
+    // weighted-triangle state
+    double* pe = nullptr;
+    double* pv = nullptr;
+    uint32_t* sup = nullptr;
+    uint8_t* st = nullptr;
+    int64_t* tl_off = nullptr;  // [m2+1]
+    rtr::TriEntry* tl = nullptr;
+    int64_t tl_len = 0;
+
+    // small device counters: [0] triangle total, [1] error word, [2..] stage stats
+    unsigned long long* ctr = nullptr;
+
+    // extraction results: clusters in creation order
+    int64_t ncl = 0;
+    int32_t* cl_seed = nullptr;    // [ncl]
+    int64_t* cl_off = nullptr;     // [ncl+1] into cl_vert
+    int32_t* cl_vert = nullptr;    // [n] members, in set-iteration order
+    int64_t* cl_ne = nullptr;      // [ncl] internal edges
+    int64_t* cl_cut = nullptr;     // [ncl] cut edges
+    int32_t* cluster_of = nullptr; // [n]
+
+    double eps = 0.3;
+    int stage = 0;  // 1 built, 2 counted, 3 cleaned, 4 extracted
+
+    // stage timings from CUDA events (ms)
+    float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0;
+    // launch accounting for this graph (kernels issued by the library)
+    long long launches = 0;
+
+    // diagnostics mirroring the reference's print-and-continue self-checks
+    long long diag_residual = 0;
+    long long diag_bad_status = 0;
+
+    std::vector<void*> owned;  // device allocations released by rtr_graph_destroy
+};
+
+namespace rtr {
+
+void* dev_alloc(rtr_graph* g, size_t bytes);  // stream-ordered, owned by g
+void dev_free_all(rtr_graph* g);
+
+// Temporary device memory released before the call returns.
+struct Scratch {
+    rtr_graph* g;
+    std::vector<void*> ptrs;
+    explicit Scratch(rtr_graph* gr) : g(gr) {}
+    void* get(size_t bytes);
+    ~Scratch();
+};
+
+int build_csr(rtr_graph* g, const int64_t* d_u, const int64_t* d_v, int64_t m, bool simplify);
+int build_csr_from_host_csr(rtr_graph* g, const int64_t* h_offsets, const int64_t* h_nbors);
+int count_triangles(rtr_graph* g);
+int initial_clean(rtr_graph* g, double eps);
+int extract_clusters(rtr_graph* g);
+
+}  // namespace rtr
