@@ -1,0 +1,381 @@
+#!/usr/bin/env python3
+"""Benchmark of the RTRExtractor decomposition path on B200.
+
+One step = one full decomposition (count + clean + extract) of the
+335,000-vertex Chung-Lu power-law graph with 2,000 planted communities
+(~926k undirected edges, seed 2; the co-purchase-network shape), at
+eps = 0.3, through librtr.so.
+
+Prints ONE JSON line (rank 0):
+  value      decomposed edges/s, whole job (all ranks), graph resident in HBM,
+             device-timed (CUDA events on the library's stream) per step,
+             L2 flushed (256 MiB write) before every step
+  e2e        the same metric through the public C ABI with host buffers:
+             pinned host edge arrays -> rtr_graph_create_from_edges (H2D +
+             device CSR build) -> rtr_decompose -> cluster_of read back (D2H)
+  roofline   the dominant kernel's algorithmic bytes / its event-timed duration
+             against the measured HBM copy bandwidth
+  cpu_baseline  the reference's own sequential RTRex (oracle/_ref/RTRex, mode s,
+             1 thread) on the same graph, or the restated oracle when that
+             binary is absent
+Multi-GPU (torchrun): replicas only -- each rank decomposes its own copy, the
+step time is the max over ranks, value counts every rank's edges.
+
+``--impl reference`` times the reference's CPU implementation instead (mode p,
+all host threads) on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "decomposed edges/s (count+clean+extract)"
+UNIT = "edges/s"
+EPS = 0.3
+WORKLOAD = "chung_lu"
+WORKLOAD_DESC = ("Chung-Lu power law n=335,000, ~926k edges, exponent 2.3, expected degree cap 550, "
+                 "+2,000 planted communities of 5-12 vertices at p=0.8, seed 2; eps=0.3")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "RTRex")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--eps", type=float, default=EPS)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from rtrex_cuda_b200 import graphgen
+    return graphgen.config_graph(WORKLOAD)
+
+
+# ------------------------------------------------------------------ CPU legs
+
+def _phase_seconds(stdout: str) -> float:
+    """count + clean + extract from the reference's phase timers (Decomposition.h:556,563,926)."""
+    keys = ["Time for getting the weights", "Time for the initial clean", "Time for getting the clusters"]
+    tot = 0.0
+    for k in keys:
+        m = re.search(re.escape(k) + r":\s*([0-9.eE+-]+)s", stdout)
+        if not m:
+            raise RuntimeError(f"reference output lacks '{k}'")
+        tot += float(m.group(1))
+    return tot
+
+
+def run_reference_binary(path: str, mode: str, threads: int) -> float:
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    with tempfile.TemporaryDirectory() as td:
+        out = subprocess.run([REF_BIN, path, "bench", repr(EPS), mode], cwd=td, env=env, capture_output=True,
+                             text=True, timeout=900)
+    if out.returncode != 0:
+        raise RuntimeError(f"reference run failed: {out.stderr[-300:]}")
+    return _phase_seconds(out.stdout)
+
+
+def run_oracle_port(n, u, v) -> float:
+    import oracle  # the restated sequential oracle, used only as a timed baseline
+    c = oracle.build_csr(n, u, v)
+    t0 = time.perf_counter()
+    s0 = oracle.count(c)
+    s1 = oracle.initial_clean(c, s0, EPS)
+    oracle.extract(c, s1, EPS)
+    return time.perf_counter() - t0
+
+
+def cpu_times(n, u, v, runs: int, mode: str, threads: int):
+    """[(seconds, kind)] for `runs` timed runs of the CPU implementation."""
+    from rtrex_cuda_b200 import graphgen
+    if os.path.exists(REF_BIN):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "g.txt")
+            graphgen.write_escape(path, n, u, v)
+            return [run_reference_binary(path, mode, threads) for _ in range(runs)], "reference"
+    return [run_oracle_port(n, u, v) for _ in range(runs)], "port"
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n, u, v = workload()
+    m = int(u.size)
+    threads = os.cpu_count() or 1
+    mode = "p"
+    cpu_times(n, u, v, args.warmup, mode, threads) if args.warmup > 0 else None
+    times, kind = cpu_times(n, u, v, args.steps, mode, threads)
+    if kind == "port":
+        threads = 1
+    sec = float(np.mean(times))
+    value = m / sec
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "desc": WORKLOAD_DESC, "n": n, "m": m, "eps": EPS},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"full decomposition of the workload graph per step, mode {mode}"
+                                   if kind == "reference" else "full decomposition, restated oracle, 1 thread"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU leg
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int, enabled: bool):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.enabled = enabled and shutil.which("nvidia-smi") is not None
+
+    def __enter__(self):
+        if self.enabled:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.th.join(timeout=2)
+
+    def summary(self):
+        if not self.enabled or not self.lines:
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def count_bytes(n, off, nb):
+    """Algorithmic bytes of the counting stage: 8(n+1) + 4*sum over the degree-
+    oriented edges (u->v) of (d+(u) + d+(v)) + 2m*12 + 8n."""
+    deg = np.diff(off)
+    src = np.repeat(np.arange(n), deg)
+    key_s = deg[src] * np.int64(n) + src
+    key_d = deg[nb] * np.int64(n) + nb
+    out = key_s < key_d  # orient from lower (deg, id) to higher
+    dplus = np.bincount(src[out], minlength=n)
+    s = int((dplus[src[out]] + dplus[nb[out]]).sum())
+    m2 = int(nb.size)
+    return 8 * (n + 1) + 4 * s + m2 * 12 + 8 * n, s
+
+
+def clean_bytes(n, off, nb, status, tri_removed):
+    """Algorithmic bytes of the clean: per removed undirected edge 4*(d(u)+d(v)),
+    one status byte per directed slot, 48 bytes per removed triangle."""
+    deg = np.diff(off)
+    src = np.repeat(np.arange(n), deg)
+    fwd = (src < nb) & (status == ord("N"))
+    return int(4 * (deg[src[fwd]] + deg[nb[fwd]]).sum() + nb.size + 48 * tri_removed)
+
+
+def ours_arm(args):
+    import torch
+    import torch.distributed as dist
+    import rtrex_cuda_b200 as rtr
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = local
+    torch.cuda.set_device(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, u, v = workload()
+    m = int(u.size)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{dev}")  # 256 MiB > 126 MB L2
+
+    def flush_l2(k):
+        flush.fill_(k)
+        torch.cuda.synchronize(dev)
+
+    g = rtr.Graph.from_edges(n, u, v, device=dev)
+    for k in range(args.warmup):
+        flush_l2(k)
+        g.decompose(args.eps)
+    launches0 = g.stats()["launches"]
+    step_ms, kms = [], []
+    barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev, not args.no_clocks) as clocks:
+        wall0 = time.perf_counter()
+        for k in range(args.steps):
+            flush_l2(k + 1)
+            ncl = g.decompose(args.eps)
+            km = g.kernel_ms()
+            step_ms.append(km["decompose"])
+            kms.append(km)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - wall0
+    barrier()
+    launches = g.stats()["launches"] - launches0
+    ms_step = allmax(float(np.mean(step_ms)))
+    value = world * m / (ms_step / 1e3)
+
+    # roofline of the dominant kernel (per-launch averages over the timed steps)
+    names = ["k_edge_fold", "k_tri_fill", "k_vertex_fold", "k_clean_units", "k_extract_components"]
+    avg = {k: float(np.mean([x[k] for x in kms])) for k in names}
+    dominant = max(names, key=lambda k: avg[k])
+    off, nb = g.csr()
+    total = g.count()
+    left = g.clean(args.eps)
+    status = g.status()
+    b_count, orient_sum = count_bytes(n, off, nb)
+    b_clean = clean_bytes(n, off, nb, status, total - left)
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(dominant)
+    if dominant == "k_clean_units":
+        alg, t_ms = b_clean, avg[dominant]
+    elif dominant in ("k_edge_fold", "k_tri_fill", "k_vertex_fold"):
+        alg, t_ms = b_count, avg["k_edge_fold"] + avg["k_tri_fill"] + avg["k_vertex_fold"]
+    else:
+        alg, t_ms = None, avg[dominant]
+    achieved = (alg / (t_ms / 1e3) / 1e9) if alg else None
+    roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "algorithmic_bytes": alg, "ms_per_launch": t_ms, "peak_kind": peak_kind}
+    t_count = avg["k_edge_fold"] + avg["k_tri_fill"] + avg["k_vertex_fold"]
+    roofline_count = {"kernels": "k_edge_fold+k_tri_fill+k_vertex_fold", "bound": "hbm",
+                      "achieved": b_count / (t_count / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                      "frac": b_count / (t_count / 1e3) / 1e9 / peak, "algorithmic_bytes": b_count,
+                      "oriented_sum": orient_sum, "ms": t_count}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.skip_e2e:
+        hu = torch.from_numpy(u).pin_memory().numpy()
+        hv = torch.from_numpy(v).pin_memory().numpy()
+        times = []
+        for k in range(args.warmup + args.steps):
+            flush_l2(k)
+            t0 = time.perf_counter()
+            g2 = rtr.Graph.from_edges(n, hu, hv, device=dev)
+            g2.decompose(args.eps)
+            cof = g2.cluster_of()
+            g2.close()
+            t1 = time.perf_counter()
+            if k >= args.warmup:
+                times.append(t1 - t0)
+        sec = allmax(float(np.mean(times)))
+        e2e = {"value": world * m / sec, "unit": UNIT, "h2d_bytes_per_step": 16 * m,
+               "d2h_bytes_per_step": int(cof.nbytes), "ms_per_step": sec * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        times, kind = cpu_times(n, u, v, 2, "s", 1)
+        sec = float(np.mean(times))
+        cpu = {"value": m / sec, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": "full decomposition of the workload graph (2 runs, mode s)" if kind == "reference"
+               else "full decomposition with the restated oracle (2 runs)",
+               "seconds_per_run": sec}
+
+    g.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "desc": WORKLOAD_DESC, "n": n, "m": m, "eps": args.eps,
+                       "clusters": ncl, "l2": "flushed (256 MiB write) before every step",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": e2e, "roofline": roofline, "roofline_count": roofline_count, "cpu_baseline": cpu,
+            "gpu_launches": launches, "kernel_ms": avg, "wall_s_timed": wall,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -114,6 +114,9 @@ int rtr_get_status(const rtr_graph* g, uint8_t* status);
 int rtr_get_clusters(const rtr_graph* g, int64_t* seed, int64_t* nv, int64_t* ne, int64_t* cut, int64_t* off,
                      int64_t* vert);
 
+/* Number of clusters produced by the last extraction (0 before one). */
+int rtr_num_clusters(const rtr_graph* g, int64_t* n_clusters);
+
 /* cluster_of[v] = index of v's cluster (creation order), the cluster_map of
  * disjointExtract (Decomposition.h:538). */
 int rtr_get_cluster_of(const rtr_graph* g, int64_t* cluster_of);
@@ -122,6 +125,13 @@ int rtr_get_cluster_of(const rtr_graph* g, int64_t* cluster_of);
  * kernel launches issued for this graph so far; diagnostic counter of the
  * reference's residual self-check (Decomposition.h:273-277). */
 int rtr_get_stats(const rtr_graph* g, double* ms4, int64_t* launches, int64_t* residual_warnings);
+
+/* Device times (ms, CUDA events on the graph's stream) of the last run of the
+ * main kernels: ms[0] edge fold, [1] triangle-list fill, [2] vertex fold,
+ * [3] unit clean replay, [4] component extraction, [5] whole rtr_decompose.
+ * Replaces: the phase timers the reference prints (Decomposition.h:556,563,926;
+ *           RTRex_CUDA/gpu_triangle_count.cu:135-139, gpu_clean.cu:206-210). */
+int rtr_get_kernel_ms(const rtr_graph* g, double* ms, int n);
 
 /* Write <name>-decomposition.txt, -stats.txt, -freq.txt and -cut.txt exactly as
  * printDecomposition does (RTRex_Sequential/clustering/RTRex.cpp:19-118,

@@ -52,7 +52,7 @@ def lib_path() -> str:
 
 
 def build(verbose: bool = False) -> str:
-    from . import build as _b
+    from . import buildlib as _b
     return _b.build(verbose)
 
 
@@ -62,7 +62,7 @@ def lib():
     if _lib is not None:
         return _lib
     if not os.path.exists(_LIB_PATH):
-        raise RtrError(-1, f"{_LIB_PATH} is missing; run python -m rtrex_cuda_b200.build")
+        raise RtrError(-1, f"{_LIB_PATH} is missing; run python -m rtrex_cuda_b200.buildlib")
     L = ctypes.CDLL(_LIB_PATH)
     P = ctypes.POINTER
     L.rtr_version.restype = ctypes.c_char_p
@@ -80,7 +80,9 @@ def lib():
     L.rtr_get_status.argtypes = [_vp, _vp]
     L.rtr_get_clusters.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.rtr_get_cluster_of.argtypes = [_vp, _vp]
+    L.rtr_num_clusters.argtypes = [_vp, P(_i64)]
     L.rtr_get_stats.argtypes = [_vp, _vp, P(_i64), P(_i64)]
+    L.rtr_get_kernel_ms.argtypes = [_vp, _vp, ctypes.c_int]
     L.rtr_write_decomposition.argtypes = [_vp, ctypes.c_char_p]
     L.rtr_load_escape.argtypes = [ctypes.c_char_p, P(_i64), P(_i64), P(_vp), P(_vp)]
     L.rtr_free.argtypes = [_vp]
@@ -220,10 +222,14 @@ class Graph:
         _check(lib().rtr_get_status(self._h, _ptr(st)))
         return st[:2 * m]
 
+    def num_clusters(self) -> int:
+        t = _i64()
+        _check(lib().rtr_num_clusters(self._h, ctypes.byref(t)))
+        return int(t.value)
+
     def clusters(self) -> Clusters:
         n = self.n
-        cof = self.cluster_of()
-        k = int(cof.max()) + 1 if n else 0
+        k = self.num_clusters()
         seed, nv, ne, cut = (np.zeros(max(1, k), np.int64) for _ in range(4))
         off = np.zeros(k + 1, np.int64)
         vert = np.zeros(max(1, n), np.int64)
@@ -241,6 +247,14 @@ class Graph:
         _check(lib().rtr_get_stats(self._h, _ptr(ms), ctypes.byref(launches), ctypes.byref(resid)))
         return {"ms_build": ms[0], "ms_count": ms[1], "ms_clean": ms[2], "ms_extract": ms[3],
                 "launches": int(launches.value), "residual_warnings": int(resid.value)}
+
+    KERNELS = ("k_edge_fold", "k_tri_fill", "k_vertex_fold", "k_clean_units", "k_extract_components", "decompose")
+
+    def kernel_ms(self) -> dict:
+        """Device times (ms) of the last run's main kernels and of the whole decompose."""
+        ms = np.zeros(8, np.float64)
+        _check(lib().rtr_get_kernel_ms(self._h, _ptr(ms), 8))
+        return {k: float(ms[i]) for i, k in enumerate(self.KERNELS)}
 
     def write_decomposition(self, name: str):
         _check(lib().rtr_write_decomposition(self._h, name.encode()))

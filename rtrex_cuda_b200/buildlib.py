@@ -1,6 +1,6 @@
 """Build librtr.so and the rtrex_b200 CLI in-tree for sm_100a.
 
-``python -m rtrex_cuda_b200.build`` (or ``__graft_entry__.build()``) compiles
+``python -m rtrex_cuda_b200.buildlib`` (or ``__graft_entry__.build()``) compiles
 every CUDA / C++ source under ``csrc/`` with nvcc for ``sm_100a`` and links
 ``rtrex_cuda_b200/librtr.so`` plus the ``rtrex_cuda_b200/rtrex_b200`` binary.
 Objects go to ``rtrex_cuda_b200/_build/``.  Floating-point contraction is

@@ -65,6 +65,15 @@ int make_graph(int64_t n, int device, rtr_graph** out)
         return RTR_ERR_CUDA;
     }
     g->own_stream = true;
+    for (int k = 0; k < 2 * rtr_graph::kTimers; ++k) cudaEventCreate(&g->kev[k]);
+    {
+        // keep freed blocks cached in the device pool between graphs
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
     g->ctr = (unsigned long long*)dev_alloc(g, 8 * sizeof(unsigned long long));
     if (!g->ctr) {
         rtr_graph_destroy(g);
@@ -172,6 +181,8 @@ int rtr_graph_destroy(rtr_graph* g)
     cudaSetDevice(g->device);
     dev_free_all(g);
     if (g->stream) cudaStreamSynchronize(g->stream);
+    for (int k = 0; k < 2 * rtr_graph::kTimers; ++k)
+        if (g->kev[k]) cudaEventDestroy(g->kev[k]);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
     delete g;
     return RTR_OK;
@@ -237,9 +248,21 @@ int rtr_extract(rtr_graph* g, int64_t* ncl)
 
 int rtr_decompose(rtr_graph* g, double eps, int64_t* ncl)
 {
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    ktime_begin(g, KT_DECOMPOSE);
     int rc = rtr_count(g, nullptr);
     if (!rc) rc = rtr_clean(g, eps, nullptr);
     if (!rc) rc = rtr_extract(g, ncl);
+    ktime_end(g, KT_DECOMPOSE);
+    if (!rc) {
+        RTR_CUDA_TRY(cudaEventSynchronize(g->kev[2 * KT_DECOMPOSE + 1]));
+        ktime_read(g, KT_DECOMPOSE);
+        g->ms_decompose = g->kms[KT_DECOMPOSE];
+    }
     return rc;
 }
 
@@ -344,6 +367,16 @@ int rtr_get_clusters(const rtr_graph* gc, int64_t* seed, int64_t* nv, int64_t* n
     return RTR_OK;
 }
 
+int rtr_num_clusters(const rtr_graph* g, int64_t* ncl)
+{
+    if (!g || !ncl) {
+        set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    *ncl = g->stage >= 4 ? g->ncl : 0;
+    return RTR_OK;
+}
+
 int rtr_get_cluster_of(const rtr_graph* gc, int64_t* cluster_of)
 {
     rtr_graph* g = const_cast<rtr_graph*>(gc);
@@ -369,6 +402,16 @@ int rtr_get_stats(const rtr_graph* g, double* ms4, int64_t* launches, int64_t* r
     }
     if (launches) *launches = g->launches;
     if (residual) *residual = g->diag_residual;
+    return RTR_OK;
+}
+
+int rtr_get_kernel_ms(const rtr_graph* g, double* ms, int n)
+{
+    if (!g || !ms) {
+        set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    for (int k = 0; k < n && k < rtr_graph::kTimers; ++k) ms[k] = g->kms[k];
     return RTR_OK;
 }
 

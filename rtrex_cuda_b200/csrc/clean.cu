@@ -370,6 +370,10 @@ int initial_clean(rtr_graph* g, double eps)
     uint32_t ns = 0;
     RTR_CUDA_TRY(cudaMemcpyAsync(&ns, d_ns, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    g->kms[KT_CLEAN_UNITS] = 0;
+    // an empty timer pair keeps the reading defined when no unit exists
+    ktime_begin(g, KT_CLEAN_UNITS);
+    ktime_end(g, KT_CLEAN_UNITS);
 
     if (ns > 0) {
         const int sbits = bits_for((uint64_t)m2);
@@ -427,14 +431,17 @@ int initial_clean(rtr_graph* g, double eps)
         int blocks = (int)std::min<int64_t>((nu + warps_per_block - 1) / warps_per_block,
                                             (int64_t)grid_for(1 << 30, kBlock, 8));
         blocks = std::max(blocks, 1);
+        ktime_begin(g, KT_CLEAN_UNITS);
         k_clean_units<<<blocks, kBlock, 0, s>>>(ca, sorted, slot_mask, units, order, nu, stacks, next_unit,
                                                 (unsigned*)(g->ctr + 1), g->ctr, g->ctr + 2);
+        ktime_end(g, KT_CLEAN_UNITS);
         g->launches += 1;
         RTR_CUDA_TRY(cudaGetLastError());
     }
     cudaEventRecord(e1, s);
     RTR_CUDA_TRY(cudaEventSynchronize(e1));
     cudaEventElapsedTime(&g->ms_clean, e0, e1);
+    if (g->kms[KT_CLEAN_UNITS] >= 0) ktime_read(g, KT_CLEAN_UNITS);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     unsigned long long h[3];

@@ -198,7 +198,9 @@ int count_triangles(rtr_graph* g)
     RTR_CUDA_TRY(cudaMemsetAsync(g->pe, 0, sizeof(double) * (m2 + 1), s));
     RTR_CUDA_TRY(cudaMemsetAsync(g->sup, 0, sizeof(uint32_t) * (m2 + 1), s));
     const int ge = grid_for(m, kBlock);
+    ktime_begin(g, KT_EDGE_FOLD);
     k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, m, g->pe, g->sup, cnt, g->ctr);
+    ktime_end(g, KT_EDGE_FOLD);
     exclusive_scan_i64(cnt, g->tl_off, m2 + 1, nullptr, tmp, s);
     g->launches += 4;
     RTR_CUDA_TRY(cudaGetLastError());
@@ -214,14 +216,21 @@ int count_triangles(rtr_graph* g)
         }
     }
     g->tl_len = tl_len;
+    ktime_begin(g, KT_TRI_FILL);
     k_tri_fill<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd, m, g->tl_off, g->tl);
+    ktime_end(g, KT_TRI_FILL);
+    ktime_begin(g, KT_VERTEX_FOLD);
     k_vertex_fold<<<grid_for(n, kBlock), kBlock, 0, s>>>(g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl,
                                                           g->pv);
+    ktime_end(g, KT_VERTEX_FOLD);
     g->launches += 2;
     RTR_CUDA_TRY(cudaGetLastError());
     cudaEventRecord(e1, s);
     RTR_CUDA_TRY(cudaEventSynchronize(e1));
     cudaEventElapsedTime(&g->ms_count, e0, e1);
+    ktime_read(g, KT_EDGE_FOLD);
+    ktime_read(g, KT_TRI_FILL);
+    ktime_read(g, KT_VERTEX_FOLD);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     g->stage = 2;

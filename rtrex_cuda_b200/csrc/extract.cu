@@ -430,7 +430,12 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
                 S.insert(cand[k].vertex);
                 a.clustered[cand[k].vertex] = 1;
             }
-            for (int64_t j = r0; j < r1; ++j) a.nbd[a.nb[j]] = 0;
+            // The reference clears the bit of every neighbour of u (Decomposition.h:879-883).
+            // Only the alive ones were set, and a dead neighbour may belong to another
+            // component that a different thread is processing right now, so clear
+            // exactly the bits this seed set.
+            for (int64_t j = r0; j < r1; ++j)
+                if (a.st[fwd_slot(u, j, a.nb, a.partner)] != ST_N) a.nbd[a.nb[j]] = 0;
 
             if (out + S.size > vb + nv || ncl >= nv) {  // clusters must partition the component
                 atomicOr(a.err, (unsigned)DEV_ERR_SCRATCH);
@@ -661,7 +666,9 @@ int extract_clusters(rtr_graph* g)
     {
         const int blk = 128;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nc + blk - 1) / blk, grid_for(1 << 30, blk, 16)));
+        ktime_begin(g, KT_EXTRACT);
         k_extract_components<<<blocks, blk, 0, s>>>(a, comps, order, nc, next_comp);
+        ktime_end(g, KT_EXTRACT);
         g->launches += 1;
     }
     RTR_CUDA_TRY(cudaGetLastError());
@@ -716,6 +723,16 @@ int extract_clusters(rtr_graph* g)
     const int gk = grid_for(ncl, kBlock);
     k_cluster_gather<<<gk, kBlock, 0, s>>>(csort, ncl, bmask, a.hdr_seed, a.hdr_size, g->cl_seed, size64);
     exclusive_scan_i64(size64, g->cl_off, ncl + 1, nullptr, ltmp, s);
+    {
+        // the clusters must partition the vertex set
+        int64_t members = -1;
+        RTR_CUDA_TRY(cudaMemcpyAsync(&members, g->cl_off + ncl, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        RTR_CUDA_TRY(cudaStreamSynchronize(s));
+        if (members != n) {
+            set_error("extraction produced %lld cluster members for %lld vertices", (long long)members, (long long)n);
+            return RTR_ERR_DEVICE;
+        }
+    }
     k_cluster_members<<<gk, kBlock, 0, s>>>(csort, ncl, bmask, a.hdr_start, g->cl_off, a.out_vert, g->cl_vert,
                                             g->cluster_of);
     RTR_CUDA_TRY(cudaMemsetAsync(g->cl_ne, 0, sizeof(int64_t) * (ncl + 1), s));
@@ -728,6 +745,7 @@ int extract_clusters(rtr_graph* g)
     cudaEventRecord(e1, s);
     RTR_CUDA_TRY(cudaEventSynchronize(e1));
     cudaEventElapsedTime(&g->ms_extract, e0, e1);
+    ktime_read(g, KT_EXTRACT);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     g->stage = 4;

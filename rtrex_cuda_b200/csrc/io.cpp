@@ -152,7 +152,7 @@ int rtr_write_decomposition(const rtr_graph* g, const char* name_c)
     std::vector<int64_t> off(n + 1), nb(2 * m), cluster_of(n);
     if ((rc = rtr_get_csr(g, off.data(), nb.data()))) return rc;
     if ((rc = rtr_get_cluster_of(g, cluster_of.data()))) return rc;
-    for (int64_t v = 0; v < n; ++v) k = std::max(k, cluster_of[v] + 1);
+    if ((rc = rtr_num_clusters(g, &k))) return rc;
     std::vector<int64_t> seed(k), nv(k), ne(k), cut(k), coff(k + 1), vert(n);
     if ((rc = rtr_get_clusters(g, seed.data(), nv.data(), ne.data(), cut.data(), coff.data(), vert.data())))
         return rc;

@@ -51,7 +51,12 @@ struct rtr_graph {
     int stage = 0;  // 1 built, 2 counted, 3 cleaned, 4 extracted
 
     // stage timings from CUDA events (ms)
-    float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0;
+    float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0, ms_decompose = 0;
+    // per-kernel device times of the last run (ms), CUDA events on the graph's stream:
+    // [0] k_edge_fold [1] k_tri_fill [2] k_vertex_fold [3] k_clean_units [4] k_extract_components
+    static constexpr int kTimers = 8;
+    cudaEvent_t kev[2 * kTimers] = {};
+    float kms[kTimers] = {};
     // launch accounting for this graph (kernels issued by the library)
     long long launches = 0;
 
@@ -65,6 +70,16 @@ struct rtr_graph {
 namespace rtr {
 
 void* dev_alloc(rtr_graph* g, size_t bytes);  // stream-ordered, owned by g
+
+// Kernel timers: record around a launch on the graph's stream, read after a sync.
+enum KernelTimer { KT_EDGE_FOLD = 0, KT_TRI_FILL, KT_VERTEX_FOLD, KT_CLEAN_UNITS, KT_EXTRACT, KT_DECOMPOSE };
+inline void ktime_begin(rtr_graph* g, int k) { cudaEventRecord(g->kev[2 * k], g->stream); }
+inline void ktime_end(rtr_graph* g, int k) { cudaEventRecord(g->kev[2 * k + 1], g->stream); }
+inline void ktime_read(rtr_graph* g, int k)
+{
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, g->kev[2 * k], g->kev[2 * k + 1]) == cudaSuccess) g->kms[k] = ms;
+}
 void dev_free_all(rtr_graph* g);
 
 // Temporary device memory released before the call returns.

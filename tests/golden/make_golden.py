@@ -1,0 +1,120 @@
+"""Regenerate tests/golden/golden.json from the reference itself.
+
+Runs the reference's own sequential code (oracle/_ref/rtr_ref_dump, compiled
+from RTRex_Sequential's sources by ``make -C oracle ref``) on every fixture
+graph and records, per stage, the reference's results:
+
+* count:   total triangles, sha256 of perEdge bits and of perVertex bits
+* clean:   triangles left, sha256 of the status bytes, perEdge bits, perVertex bits
+* extract: number of clusters and sha256 of the cluster list (creation order,
+           "nv ne cut : members" in set-iteration order, one line per cluster)
+* files:   sha256 of RTRex-<name>-{decomposition,stats,freq,cut}.txt written by
+           the reference CLI (oracle/_ref/RTRex <graph> <name> <eps> s)
+
+small_test (the reference's RTRex_Sequential/Example/small-test.txt graph)
+additionally stores full arrays in small_test.npz.  Graph inputs are either
+regenerated from seeds (rtrex_cuda_b200.graphgen) or, for the bundled data
+files, read from the reference checkout (those cases skip when it is absent).
+
+Usage: python tests/golden/make_golden.py [--reference /root/reference]
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from rtrex_cuda_b200 import graphgen  # noqa: E402
+from tests.golden.cases import CASES, BUNDLED, load_case  # noqa: E402
+
+
+def sha(b: bytes) -> str:
+    return hashlib.sha256(b).hexdigest()
+
+
+def cluster_text_from_lines(lines):
+    return ("\n".join(lines) + "\n").encode()
+
+
+def run_reference(dump_bin: str, path: str, eps: float):
+    with tempfile.TemporaryDirectory() as td:
+        subprocess.run([dump_bin, path, repr(eps), td], check=True, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+        rd = lambda f, dt: np.fromfile(os.path.join(td, f), dtype=dt)
+        out = {
+            "count": {
+                "total": int(rd("count_total.i64", np.int64)[0]),
+                "perEdge": sha(rd("count_perEdge.f64", np.uint64).tobytes()),
+                "perVertex": sha(rd("count_perVertex.f64", np.uint64).tobytes()),
+            },
+            "clean": {
+                "total": int(rd("clean_total.i64", np.int64)[0]),
+                "status": sha(rd("clean_status.u8", np.uint8).tobytes()),
+                "perEdge": sha(rd("clean_perEdge.f64", np.uint64).tobytes()),
+                "perVertex": sha(rd("clean_perVertex.f64", np.uint64).tobytes()),
+            },
+        }
+        lines = open(os.path.join(td, "clusters.txt")).read().splitlines()
+        out["extract"] = {"clusters": len(lines), "digest": sha(cluster_text_from_lines(lines))}
+        arrays = {k: rd(f, dt) for k, f, dt in [
+            ("offsets", "csr_offsets.i64", np.int64), ("nbors", "csr_nbors.i64", np.int64),
+            ("count_perEdge", "count_perEdge.f64", np.float64), ("count_perVertex", "count_perVertex.f64", np.float64),
+            ("clean_status", "clean_status.u8", np.uint8), ("clean_perEdge", "clean_perEdge.f64", np.float64),
+            ("clean_perVertex", "clean_perVertex.f64", np.float64)]}
+        arrays["clusters"] = np.array(lines)
+        return out, arrays
+
+
+def run_reference_cli(cli_bin: str, path: str, eps: float):
+    """sha256 of the four files RTRex <graph> <name> <eps> s writes (RTRex.cpp:194)."""
+    with tempfile.TemporaryDirectory() as td:
+        subprocess.run([cli_bin, path, "g", repr(eps), "s"], check=True, cwd=td, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+        return {kind: sha(open(os.path.join(td, f"RTRex-g-{kind}.txt"), "rb").read())
+                for kind in ("decomposition", "stats", "freq", "cut")}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    dump_bin = os.path.join(ROOT, "oracle", "_ref", "rtr_ref_dump")
+    if not os.path.exists(dump_bin):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.reference}"], check=True)
+    golden = {"eps": {}, "cases": {}}
+    with tempfile.TemporaryDirectory() as td:
+        for name, eps_list in CASES.items():
+            if name in BUNDLED:
+                path = os.path.join(args.reference, BUNDLED[name])
+                if not os.path.exists(path):
+                    print("skip", name)
+                    continue
+            else:
+                n, u, v = load_case(name)
+                path = os.path.join(td, name + ".txt")
+                graphgen.write_escape(path, n, u, v)
+            entry = {}
+            for eps in eps_list:
+                res, arrays = run_reference(dump_bin, path, eps)
+                res["files"] = run_reference_cli(os.path.join(ROOT, "oracle", "_ref", "RTRex"), path, eps)
+                entry[repr(eps)] = res
+                if name == "small_test" and eps == 0.3:
+                    np.savez_compressed(os.path.join(HERE, "small_test.npz"), **arrays)
+                print(name, eps, res["count"]["total"], res["clean"]["total"], res["extract"]["clusters"], flush=True)
+            golden["cases"][name] = entry
+    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        json.dump(golden, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()

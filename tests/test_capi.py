@@ -1,0 +1,96 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol rtr.h
+declares, parses Escape files with the reference loader's rules, and fails
+loudly (no CPU fallback) when no CUDA device is present."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import rtrex_cuda_b200 as rtr
+from tests import helpers
+
+
+def _declared_functions():
+    text = open(os.path.join(helpers.ROOT, "include", "rtr.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rtr_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = _declared_functions()
+    assert len(names) >= 18
+    L = rtr.lib()
+    for nm in names:
+        assert hasattr(L, nm), f"librtr.so does not export {nm}"
+    out = subprocess.run(["nm", "-D", "--defined-only", rtr.lib_path()], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (rtr_[a-z0-9_]+)", out))
+    assert set(names) <= exported
+
+
+def test_version():
+    assert b"sm_100a" in rtr.lib().rtr_version()
+
+
+def _write(tmp_path, text):
+    p = tmp_path / "g.txt"
+    p.write_text(text)
+    return str(p)
+
+
+def test_escape_parser_rules(tmp_path):
+    # comments and blank lines are skipped; the first data line is "n m"
+    p = _write(tmp_path, "# header comment\n\n4 3\n0 1\n# mid comment\n1 2\n   \n2 3\n")
+    n, u, v = rtr.load_escape(p)
+    assert n == 4 and u.tolist() == [0, 1, 2] and v.tolist() == [1, 2, 3]
+
+
+def test_escape_parser_short_file(tmp_path):
+    # fewer edges than declared -> the reference's ecIOError (GraphIO.cpp:67-71)
+    p = _write(tmp_path, "5 4\n0 1\n1 2\n")
+    with pytest.raises(rtr.RtrError) as e:
+        rtr.load_escape(p)
+    assert e.value.code == 7 and "expected 8 edges, only got 4" in str(e.value)
+
+
+def test_escape_parser_missing_file(tmp_path):
+    with pytest.raises(rtr.RtrError) as e:
+        rtr.load_escape(str(tmp_path / "nope.txt"))
+    assert e.value.code == 7
+
+
+def test_escape_parser_malformed(tmp_path):
+    p = _write(tmp_path, "3 2\n0 1\nx y\n")
+    with pytest.raises(rtr.RtrError):
+        rtr.load_escape(p)
+
+
+def test_escape_parser_matches_graphgen_writer(tmp_path):
+    from rtrex_cuda_b200 import graphgen
+    n, u, v = graphgen.sbm(2000, 4001)
+    p = str(tmp_path / "s.txt")
+    graphgen.write_escape(p, n, u, v)
+    n2, u2, v2 = rtr.load_escape(p)
+    assert n2 == n and (u2 == u).all() and (v2 == v).all()
+
+
+def test_no_cpu_fallback_without_gpu():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(rtr.RtrError) as e:
+        rtr.Graph.from_edges(3, np.array([0, 1]), np.array([1, 2]))
+    assert e.value.code == 2 and "no CUDA device" in str(e.value)
+
+
+def test_null_arguments_rejected():
+    L = rtr.lib()
+    assert L.rtr_count(None, None) == 1
+    assert L.rtr_graph_destroy(None) == 0
+    h = ctypes.c_void_p()
+    assert L.rtr_graph_create_from_edges(None, None, 5, 3, 0, 0, ctypes.byref(h)) == 1
