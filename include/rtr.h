@@ -133,6 +133,26 @@ int rtr_get_stats(const rtr_graph* g, double* ms4, int64_t* launches, int64_t* r
  *           RTRex_CUDA/gpu_triangle_count.cu:135-139, gpu_clean.cu:206-210). */
 int rtr_get_kernel_ms(const rtr_graph* g, double* ms, int n);
 
+/* Weighted triangle counting into caller-provided DEVICE buffers, with no
+ * device allocation at all -- for callers that cannot let a library call
+ * cudaMalloc (a server that reserves its HBM budget up front and allocates only
+ * from its own arena, or a latency-critical path where cudaMalloc/cudaFree may
+ * synchronise the device).  No counterpart in the reference: it is an extra
+ * entry point of this library.
+ *   d_offsets int64[n+1], d_nbors int32[2m]  symmetric CSR on the current device,
+ *                                            rows strictly ascending
+ *   d_perEdge f64[2m], d_perVertex f64[n], d_support u32[2m], d_total int64[1]
+ *                                            outputs, bit-identical to rtr_count's
+ *   stream    a cudaStream_t (NULL = the default stream); the call is
+ *             asynchronous and the outputs are ready when the stream is
+ * Working memory is one fixed static device array (about 4.2 MB, held by every
+ * GPU that loads librtr.so until exit), so n is limited to 1,048,576 vertices;
+ * larger graphs get RTR_ERR_LIMIT.  The first call on each device looks up that
+ * array's device address (make it before any stream capture).  All calls share
+ * the array, so calls that overlap on the GPU race: serialise them. */
+int rtr_count_noalloc(const int64_t* d_offsets, const int32_t* d_nbors, int64_t n, double* d_perEdge,
+                      double* d_perVertex, uint32_t* d_support, int64_t* d_total, void* stream);
+
 /* Write <name>-decomposition.txt, -stats.txt, -freq.txt and -cut.txt exactly as
  * printDecomposition does (RTRex_Sequential/clustering/RTRex.cpp:19-118,
  * RTRex_CUDA/main.cu:57-108), and print its summary lines to stdout. */
