@@ -6,8 +6,8 @@
 // (no 'N' edge), subtracting the triangle weight from the two other edges and
 // the three vertices, and pushes the other edges that fall below threshold.
 // Floating-point sums make the survivor set depend on that exact order (a
-// bulk-synchronous peel differs on the bundled email / astro graphs), so the
-// device replays the same order -- but only where order can matter:
+// bulk-synchronous peel differs on order-sensitive inputs), so the device
+// replays the same order -- but only where order can matter:
 //
 //  * a seed with no triangles is a no-op pop: it is marked 'N' directly;
 //  * edges with triangles split into vertex-disjoint units (connected
@@ -18,11 +18,16 @@
 //    replay its own seeds (in slot order, popped last-first) and cascades
 //    independently and still perform the reference's operations, in the
 //    reference's order, on every cell;
-//  * one warp replays one unit: per popped edge the lanes take 32 triangles of
-//    the edge's triangle list at a time, update the distinct per-triangle
-//    cells in parallel, fold the shared cells (the popped edge, its two
-//    endpoints) in triangle order, and append pushes in the reference's push
-//    order (triangle order, (lower,w) before (higher,w)).
+//  * one warp replays one unit.  A pop is latency-bound, so its data is laid
+//    out for two dependent round trips: (1) the popped edge's 32-byte record
+//    and its triangle-list entries (which carry the triangle weight), then
+//    (2) the records of the two other edges of every triangle and the third
+//    vertex's weight.  The lanes take 32 triangles at a time, update the
+//    distinct per-triangle cells in parallel, fold the shared cells (the
+//    popped edge, its two endpoints) in triangle order, and append pushes in
+//    the reference's push order (triangle order, (lower,w) before (higher,w)).
+//    Seeds are loaded 32 at a time; support only decreases, so a seed whose
+//    support is already 0 when loaded is retired without a pop.
 #include "primitives.cuh"
 #include "rtr_graph.cuh"
 
@@ -35,28 +40,57 @@ namespace {
 
 constexpr int kBlock = 256;
 
+__device__ __forceinline__ uint8_t status_char(uint32_t ss)
+{
+    const uint32_t c = ss & SS_CODE;
+    return c == SS_N ? ST_N : (c == SS_S ? ST_S : ST_Y);
+}
+
+// Seeding pass over the forward edges (Decomposition.h:378-405) and the
+// construction of the clean-time edge records.
 __global__ void k_seed(const int32_t* __restrict__ esrc, const int32_t* __restrict__ nb,
                        const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd, int64_t m, double eps,
-                       const double* __restrict__ pe, const uint32_t* __restrict__ sup, uint8_t* __restrict__ st,
-                       uint32_t* __restrict__ is_seed)
+                       const double* __restrict__ pe, const uint32_t* __restrict__ sup,
+                       const int64_t* __restrict__ tl_off, EdgeRec* __restrict__ rec, uint32_t* __restrict__ is_seed,
+                       unsigned* __restrict__ err)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = fwd[k];
         const int64_t du = deg[esrc[i]], dv = deg[nb[i]];
-        const double ew = 1 / (double)(du * dv);
-        const bool below = pe[i] < eps * ew;
-        uint8_t s = ST_Y;
-        uint32_t seed = 0;
-        if (below) {
-            if (sup[i] > 0) {
-                s = ST_S;
+        const double thr = eps * (1 / (double)(du * dv));
+        const double p = pe[i];
+        const uint32_t s = sup[i];
+        if (s > SS_SUP) atomicOr(err, (unsigned)DEV_ERR_SCRATCH);
+        uint32_t code = SS_Y, seed = 0;
+        if (p < thr) {
+            if (s > 0) {
+                code = SS_S;
                 seed = 1;
             } else {
-                s = ST_N;  // a pop with no triangle changes nothing but its own status
+                code = SS_N;  // a pop with no triangle changes nothing but its own status
             }
         }
-        st[i] = s;
+        EdgeRec r;
+        r.pe = p;
+        r.thr = thr;
+        r.t0 = tl_off[i];
+        r.cnt = (uint32_t)(tl_off[i + 1] - r.t0);
+        r.ss = (s & SS_SUP) | code;
+        rec[k] = r;
         is_seed[k] = seed;
+    }
+}
+
+// Write the records back into the slot-indexed arrays the other stages use.
+__global__ void k_clean_finish(const int32_t* __restrict__ fwd, int64_t m, const EdgeRec* __restrict__ rec,
+                               double* __restrict__ pe, uint32_t* __restrict__ sup, uint8_t* __restrict__ st)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = fwd[k];
+        const EdgeRec r = rec[k];
+        pe[i] = r.pe;
+        sup[i] = r.ss & SS_SUP;
+        st[i] = status_char(r.ss);
     }
 }
 
@@ -122,21 +156,20 @@ __global__ void k_unit_edges(const int32_t* __restrict__ esrc, const int32_t* __
     }
 }
 
+// Seed key = (unit root, forward rank): sorting groups seeds by unit and keeps
+// slot order inside a unit (forward ranks ascend with slots).
 __global__ void k_seed_keys(const int32_t* __restrict__ fwd, const int32_t* __restrict__ esrc,
                             const uint32_t* __restrict__ is_seed, const uint32_t* __restrict__ pos, int64_t m,
-                            const int32_t* __restrict__ root, int sbits, uint64_t* __restrict__ keys)
+                            const int32_t* __restrict__ root, int rbits, uint64_t* __restrict__ keys)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
-        if (is_seed[k]) {
-            const int64_t i = fwd[k];
-            keys[pos[k]] = ((uint64_t)root[esrc[i]] << sbits) | (uint64_t)i;
-        }
+        if (is_seed[k]) keys[pos[k]] = ((uint64_t)root[esrc[fwd[k]]] << rbits) | (uint64_t)k;
 }
 
-__global__ void k_unit_heads(const uint64_t* __restrict__ keys, int64_t ns, int sbits, uint32_t* __restrict__ head)
+__global__ void k_unit_heads(const uint64_t* __restrict__ keys, int64_t ns, int rbits, uint32_t* __restrict__ head)
 {
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < ns; j += (int64_t)gridDim.x * blockDim.x)
-        head[j] = (j == 0 || (keys[j] >> sbits) != (keys[j - 1] >> sbits)) ? 1u : 0u;
+        head[j] = (j == 0 || (keys[j] >> rbits) != (keys[j - 1] >> rbits)) ? 1u : 0u;
 }
 
 struct UnitDesc {
@@ -146,7 +179,7 @@ struct UnitDesc {
     int64_t stack_cap;
 };
 
-__global__ void k_unit_desc(const uint64_t* __restrict__ keys, int64_t ns, int sbits,
+__global__ void k_unit_desc(const uint64_t* __restrict__ keys, int64_t ns, int rbits,
                             const uint32_t* __restrict__ head, const uint32_t* __restrict__ hpos,
                             const uint32_t* __restrict__ ecount, UnitDesc* __restrict__ units,
                             int64_t* __restrict__ cap)
@@ -155,8 +188,7 @@ __global__ void k_unit_desc(const uint64_t* __restrict__ keys, int64_t ns, int s
         if (!head[j]) continue;
         const uint32_t u = hpos[j];
         units[u].seed_begin = j;
-        const uint32_t r = (uint32_t)(keys[j] >> sbits);
-        cap[u] = ecount[r];
+        cap[u] = ecount[(uint32_t)(keys[j] >> rbits)];
     }
 }
 
@@ -170,157 +202,236 @@ __global__ void k_unit_finish(UnitDesc* __restrict__ units, const int64_t* __res
         units[u].stack_cap = cap[u];
         // schedule units with the most seeds first
         const uint64_t work = (uint64_t)(units[u].seed_end - units[u].seed_begin);
-        order_keys[u] = ((uint64_t)(0xffffffffu - (uint32_t)(work < 0xffffffffull ? work : 0xffffffffull)) << 32) | (uint64_t)u;
+        order_keys[u] = ((uint64_t)(0xffffffffu - (uint32_t)(work < 0xffffffffull ? work : 0xffffffffull)) << 32) |
+                        (uint64_t)u;
     }
 }
 
+// One cascade-stack entry: the pair as deleteAndClean pushed it plus the
+// static data its pop needs (degrees, triangle-list bounds), so a pop issues
+// no lookups before its first dynamic load.  Seeds use the same descriptor.
 struct StackEntry {
-    int32_t e;      // forward slot of the edge
-    int32_t first;  // Pair.first  (deleteAndClean's u)
-    int32_t second; // Pair.second (deleteAndClean's v)
-    int32_t pad;
+    int32_t e;        // forward rank of the edge
+    int32_t first;    // Pair.first  (deleteAndClean's u)
+    int32_t second;   // Pair.second (deleteAndClean's v)
+    int32_t dfirst;   // deg(first)
+    int32_t dsecond;  // deg(second)
+    int32_t cnt;      // triangle-list length
+    int64_t t0;       // triangle-list start
 };
+static_assert(sizeof(StackEntry) == 32, "StackEntry is 32 bytes");
+
+// Seed descriptors, sorted seed j (unit-major, slot order within a unit).
+__global__ void k_seed_info(const uint64_t* __restrict__ keys, int64_t ns, uint64_t rmask,
+                            const int32_t* __restrict__ fwd, const int32_t* __restrict__ esrc,
+                            const int32_t* __restrict__ nb, const int32_t* __restrict__ deg,
+                            const EdgeRec* __restrict__ rec, StackEntry* __restrict__ info)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < ns; j += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t k = (int32_t)(keys[j] & rmask);
+        const int64_t i = fwd[k];
+        const int32_t u = esrc[i], v = nb[i];  // seeds are pushed as (u, v) with u < v
+        info[j] = StackEntry{k, u, v, deg[u], deg[v], (int32_t)rec[k].cnt, rec[k].t0};
+    }
+}
 
 struct CleanArgs {
-    const int64_t* off;
-    const int32_t* nb;
-    const int32_t* esrc;
-    const int32_t* deg;
-    const int64_t* tl_off;
     const TriEntry* tl;
-    double* pe;
+    EdgeRec* rec;
     double* pv;
-    uint32_t* sup;
-    uint8_t* st;
-    double eps;
     double inv_n;
+    const StackEntry* seeds;
+};
+
+constexpr int kCleanBlock = 128;
+constexpr int kCleanWarps = kCleanBlock / 32;
+constexpr int kSmemStack = 256;  // newest stack entries of each warp live in shared memory
+
+// Per-warp cascade stack: the newest entries in shared memory, older ones
+// spilled in order to the unit's global region (LIFO order is preserved).
+struct WarpStack {
+    StackEntry* sm;  // kSmemStack entries
+    StackEntry* gm;  // unit's global region
+    int64_t gtop;
+    int64_t cap;
+    int scount;
 };
 
 // Pop one edge: deleteAndClean's loop body (Decomposition.h:152-281) for the
-// whole warp.  Returns the number of triangles removed.
-__device__ __forceinline__ int pop_edge(const CleanArgs& a, int32_t e, int32_t u, int32_t v, StackEntry* stack,
-                                        int64_t& top, int64_t cap, unsigned* err, unsigned long long* diag)
+// whole warp.  Returns the number of triangles removed, or -1 on overflow.
+__device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c, WarpStack& ws, double* sw,
+                                        unsigned* err, unsigned long long* diag)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    const uint32_t s_e = a.sup[e];
+    const int32_t e = c.e, u = c.first, v = c.second;
+    const int32_t du = c.dfirst, dv = c.dsecond;
+    // round trip 1: the edge's record, its endpoints' weights, its first 32 triangles
+    uint32_t s_e = 0;
+    double scal = 0.0;
+    if (lane == 0) s_e = a.rec[e].ss;
+    else if (lane == 1) scal = a.rec[e].pe;
+    else if (lane == 2) scal = a.pv[u];
+    else if (lane == 3) scal = a.pv[v];
+    TriEntry t{};
+    if (lane < c.cnt) t = a.tl[c.t0 + lane];
+    s_e = __shfl_sync(0xffffffffu, s_e, 0) & SS_SUP;
+    double acc_e = __shfl_sync(0xffffffffu, scal, 1);
+    double acc_u = __shfl_sync(0xffffffffu, scal, 2);
+    double acc_v = __shfl_sync(0xffffffffu, scal, 3);
     if (s_e == 0) {
-        __syncwarp();
         if (lane == 0) {
-            if (fabs(a.pe[e]) > a.inv_n) atomicAdd(&diag[0], 1ull);
-            a.st[e] = ST_N;
+            if (fabs(acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
+            a.rec[e].ss = SS_N;
         }
         __syncwarp();
         return 0;
     }
-    const int64_t du = a.deg[u], dv = a.deg[v];
     const bool lo_is_u = du < dv;
     const int32_t lower = lo_is_u ? u : v;
     const int32_t higher = lo_is_u ? v : u;
-    const int64_t dlow = lo_is_u ? du : dv;
-    const int64_t dhigh = lo_is_u ? dv : du;
-    const bool lower_is_a = lower == a.esrc[e];  // a = smaller endpoint of the forward slot
-    const int64_t t0 = a.tl_off[e], t1 = a.tl_off[e + 1];
-    double acc_e = a.pe[e], acc_u = a.pv[u], acc_v = a.pv[v];
-    const int64_t duv = du * dv;
+    const int32_t dlow = lo_is_u ? du : dv;
+    const int32_t dhigh = lo_is_u ? dv : du;
+    const bool lower_is_a = lower == (u < v ? u : v);  // a = smaller endpoint of the forward edge
     int removed = 0;
-    for (int64_t base = t0; base < t1; base += 32) {
-        const int64_t idx = base + lane;
-        const bool valid = idx < t1;
-        TriEntry t = {0, 0, 0, 1};
-        if (valid) t = a.tl[idx];
-        const int32_t elw = lower_is_a ? t.eaz : t.ebz;
-        const int32_t ehw = lower_is_a ? t.ebz : t.eaz;
-        uint8_t slw = ST_N, shw = ST_N;
+    for (int base = 0; base < c.cnt; base += 32) {
+        const bool valid = base + lane < c.cnt;
+        if (base > 0) t = valid ? a.tl[c.t0 + base + lane] : TriEntry{};
+        const int32_t rlw = lower_is_a ? t.raz : t.rbz;
+        const int32_t rhw = lower_is_a ? t.rbz : t.raz;
+        // round trip 2: both other edges' records and the third vertex's weight
+        EdgeRec r1{}, r2{};
+        r1.ss = SS_N;
+        r2.ss = SS_N;
+        double pz = 0.0;
         if (valid) {
-            slw = a.st[elw];
-            shw = a.st[ehw];
+            r1 = a.rec[rlw];
+            r2 = a.rec[rhw];
+            pz = a.pv[t.z];
         }
-        const bool live = valid && slw != ST_N && shw != ST_N;
-        double wgt = 0.0;
+        const uint32_t c1 = r1.ss & SS_CODE, c2 = r2.ss & SS_CODE;
+        const bool live = valid && c1 != SS_N && c2 != SS_N;
+        const double wgt = live ? t.wgt : 0.0;
         bool p1 = false, p2 = false;
         if (live) {
-            wgt = 1 / (double)(duv * (int64_t)t.dz);
-            const double x1 = a.pe[elw] - wgt;
-            const double x2 = a.pe[ehw] - wgt;
-            a.pe[elw] = x1;
-            a.pe[ehw] = x2;
-            a.sup[elw] -= 1u;
-            a.sup[ehw] -= 1u;
-            a.pv[t.z] -= wgt;
-            p1 = slw != ST_S && x1 < a.eps * (1 / (double)(dlow * (int64_t)t.dz));
-            p2 = shw != ST_S && x2 < a.eps * (1 / (double)(dhigh * (int64_t)t.dz));
-            if (p1) a.st[elw] = ST_S;
-            if (p2) a.st[ehw] = ST_S;
+            const double x1 = r1.pe - wgt;
+            const double x2 = r2.pe - wgt;
+            p1 = c1 != SS_S && x1 < r1.thr;
+            p2 = c2 != SS_S && x2 < r2.thr;
+            a.rec[rlw].pe = x1;
+            a.rec[rhw].pe = x2;
+            a.rec[rlw].ss = ((r1.ss & SS_SUP) - 1u) | (p1 ? SS_S : c1);
+            a.rec[rhw].ss = ((r2.ss & SS_SUP) - 1u) | (p2 ? SS_S : c2);
+            a.pv[t.z] = pz - wgt;
         }
+        sw[lane] = wgt;
         const unsigned lm = __ballot_sync(0xffffffffu, live);
         const unsigned b1 = __ballot_sync(0xffffffffu, p1);
         const unsigned b2 = __ballot_sync(0xffffffffu, p2);
+        __syncwarp();
         // the popped edge and its endpoints accumulate in triangle order
         for (unsigned mm = lm; mm; mm &= mm - 1) {
-            const double w = __shfl_sync(0xffffffffu, wgt, __ffs(mm) - 1);
+            const double w = sw[__ffs(mm) - 1];
             acc_e -= w;
             acc_u -= w;
             acc_v -= w;
         }
         const int np = __popc(b1) + __popc(b2);
-        if (top + np > cap) {
-            if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_STACK_OVERFLOW);
-            return -1;
+        if (np) {
+            if (ws.scount + np > kSmemStack) {  // spill the shared part, oldest first
+                if (ws.gtop + ws.scount > ws.cap) {
+                    if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                    return -1;
+                }
+                for (int k = lane; k < ws.scount; k += 32) ws.gm[ws.gtop + k] = ws.sm[k];
+                ws.gtop += ws.scount;
+                ws.scount = 0;
+                __syncwarp();
+            }
+            const int before = ws.scount + __popc(b1 & lt) + __popc(b2 & lt);
+            if (p1) ws.sm[before] = StackEntry{rlw, lower, t.z, dlow, t.dz, (int32_t)r1.cnt, r1.t0};
+            if (p2) ws.sm[before + (p1 ? 1 : 0)] = StackEntry{rhw, higher, t.z, dhigh, t.dz, (int32_t)r2.cnt, r2.t0};
+            ws.scount += np;
         }
-        const int before = __popc(b1 & lt) + __popc(b2 & lt);
-        if (p1) stack[top + before] = StackEntry{elw, lower, t.z, 0};
-        if (p2) stack[top + before + (p1 ? 1 : 0)] = StackEntry{ehw, higher, t.z, 0};
-        top += np;
+        __syncwarp();
         removed += __popc(lm);
     }
-    __syncwarp();
     if (lane == 0) {
-        a.pe[e] = acc_e;
+        a.rec[e].pe = acc_e;
+        a.rec[e].ss = (s_e - (uint32_t)removed) | SS_N;
         a.pv[u] = acc_u;
         a.pv[v] = acc_v;
-        a.sup[e] = s_e - (uint32_t)removed;
         if (fabs(acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
-        a.st[e] = ST_N;
     }
     __syncwarp();
     return removed;
 }
 
-__global__ void __launch_bounds__(kBlock)
-    k_clean_units(CleanArgs a, const uint64_t* __restrict__ seed_keys, uint64_t slot_mask,
-                  const UnitDesc* __restrict__ units, const uint64_t* __restrict__ order, int64_t nu,
+__global__ void __launch_bounds__(kCleanBlock)
+    k_clean_units(CleanArgs a, const UnitDesc* __restrict__ units, const uint64_t* __restrict__ order, int64_t nu,
                   StackEntry* __restrict__ stacks, unsigned* __restrict__ next_unit, unsigned* __restrict__ err,
                   unsigned long long* __restrict__ total, unsigned long long* __restrict__ diag)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ StackEntry s_stack[kCleanWarps][kSmemStack];
+    __shared__ double s_w[kCleanWarps][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double* sw = s_w[wid];
     while (true) {
         unsigned ui = 0;
         if (lane == 0) ui = atomicAdd(next_unit, 1u);
         ui = __shfl_sync(0xffffffffu, ui, 0);
         if ((int64_t)ui >= nu) break;
         const UnitDesc ud = units[(uint32_t)order[ui]];
-        StackEntry* stack = stacks + ud.stack_base;
-        int64_t top = 0;
-        int64_t sp = ud.seed_end;
+        WarpStack ws{s_stack[wid], stacks + ud.stack_base, 0, ud.stack_cap, 0};
+        int64_t sp = ud.seed_end;  // seeds [seed_begin, sp) not yet loaded
+        // Window of the next 32 seeds in pop order (lane k = seed sp_at_load-1-k).
+        unsigned wmask = 0;
+        StackEntry wseed{};
         unsigned long long removed = 0;
         while (true) {
-            int32_t e, u, v;
-            if (top > 0) {
-                --top;
-                const StackEntry se = stack[top];
-                e = se.e;
-                u = se.first;
-                v = se.second;
-            } else if (sp > ud.seed_begin) {
-                --sp;
-                e = (int32_t)(seed_keys[sp] & slot_mask);
-                u = a.esrc[e];  // seeds are pushed as (u, v) with u < v
-                v = a.nb[e];
+            StackEntry cur;
+            if (ws.scount > 0) {
+                cur = ws.sm[--ws.scount];
+            } else if (ws.gtop > 0) {
+                const int k = (int)(ws.gtop < kSmemStack ? ws.gtop : kSmemStack);
+                for (int j = lane; j < k; j += 32) ws.sm[j] = ws.gm[ws.gtop - k + j];
+                ws.gtop -= k;
+                ws.scount = k;
+                __syncwarp();
+                cur = ws.sm[--ws.scount];
             } else {
-                break;
+                if (wmask == 0) {
+                    if (sp <= ud.seed_begin) break;
+                    const int64_t lo = (sp - 32 > ud.seed_begin) ? sp - 32 : ud.seed_begin;
+                    const int wn = (int)(sp - lo);
+                    bool live_seed = false;
+                    if (lane < wn) {
+                        wseed = a.seeds[sp - 1 - lane];
+                        const EdgeRec r = a.rec[wseed.e];
+                        // Support only decreases: a seed already at 0 is a no-op pop.
+                        live_seed = (r.ss & SS_SUP) > 0;
+                        if (!live_seed) {
+                            if (fabs(r.pe) > a.inv_n) atomicAdd(&diag[0], 1ull);
+                            a.rec[wseed.e].ss = SS_N;
+                        }
+                    }
+                    wmask = __ballot_sync(0xffffffffu, live_seed);
+                    sp = lo;
+                    __syncwarp();
+                    if (wmask == 0) continue;
+                }
+                const int k = __ffs(wmask) - 1;
+                wmask &= wmask - 1;
+                cur.e = __shfl_sync(0xffffffffu, wseed.e, k);
+                cur.first = __shfl_sync(0xffffffffu, wseed.first, k);
+                cur.second = __shfl_sync(0xffffffffu, wseed.second, k);
+                cur.dfirst = __shfl_sync(0xffffffffu, wseed.dfirst, k);
+                cur.dsecond = __shfl_sync(0xffffffffu, wseed.dsecond, k);
+                cur.cnt = __shfl_sync(0xffffffffu, wseed.cnt, k);
+                cur.t0 = __shfl_sync(0xffffffffu, wseed.t0, k);
             }
-            const int r = pop_edge(a, e, u, v, stack, top, ud.stack_cap, err, diag);
+            __syncwarp();
+            const int r = pop_edge(a, cur, ws, sw, err, diag);
             if (r < 0) break;
             removed += (unsigned long long)r;
         }
@@ -351,14 +462,16 @@ int initial_clean(rtr_graph* g, double eps)
     uint32_t* d_ns = (uint32_t*)sc.get(sizeof(uint32_t) * 2);
     int32_t* root = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
     uint32_t* ecount = (uint32_t*)sc.get(sizeof(uint32_t) * (n + 1));
-    if (!is_seed || !spos || !stmp || !d_ns || !root || !ecount) {
+    EdgeRec* rec = (EdgeRec*)sc.get(sizeof(EdgeRec) * (m + 1));
+    if (!is_seed || !spos || !stmp || !d_ns || !root || !ecount || !rec) {
         set_error("device allocation failed (clean)");
         return RTR_ERR_CUDA;
     }
     RTR_CUDA_TRY(cudaMemsetAsync(g->ctr + 1, 0, 2 * sizeof(unsigned long long), s));
     RTR_CUDA_TRY(cudaMemsetAsync(g->st, ST_N, m2 + 16, s));  // backward slots are never read
     const int gm = grid_for(m, kBlock), gn = grid_for(n, kBlock);
-    k_seed<<<gm, kBlock, 0, s>>>(g->esrc, g->nbors, g->deg, g->fwd, m, eps, g->pe, g->sup, g->st, is_seed);
+    k_seed<<<gm, kBlock, 0, s>>>(g->esrc, g->nbors, g->deg, g->fwd, m, eps, g->pe, g->sup, g->tl_off, rec, is_seed,
+                                 (unsigned*)(g->ctr + 1));
     k_uf_init<<<gn, kBlock, 0, s>>>(root, n);
     k_uf_hook_support<<<gm, kBlock, 0, s>>>(g->esrc, g->nbors, g->fwd, m, g->sup, root);
     k_uf_flatten<<<gn, kBlock, 0, s>>>(root, n);
@@ -376,23 +489,26 @@ int initial_clean(rtr_graph* g, double eps)
     ktime_end(g, KT_CLEAN_UNITS);
 
     if (ns > 0) {
-        const int sbits = bits_for((uint64_t)m2);
+        const int rbits = bits_for((uint64_t)m);
+        const uint64_t rmask = (1ull << rbits) - 1;
         uint64_t* keys = (uint64_t*)sc.get(sizeof(uint64_t) * (ns + 1));
         uint64_t* alt = (uint64_t*)sc.get(sizeof(uint64_t) * (ns + 1));
         void* rtmp = sc.get(radix_temp_bytes(ns));
         uint32_t* head = (uint32_t*)sc.get(sizeof(uint32_t) * (ns + 1));
         uint32_t* hpos = (uint32_t*)sc.get(sizeof(uint32_t) * (ns + 1));
         uint32_t* htmp = (uint32_t*)sc.get(sizeof(uint32_t) * scan_temp_elems(ns + 1));
-        if (!keys || !alt || !rtmp || !head || !hpos || !htmp) {
+        StackEntry* seeds = (StackEntry*)sc.get(sizeof(StackEntry) * (ns + 1));
+        if (!keys || !alt || !rtmp || !head || !hpos || !htmp || !seeds) {
             set_error("device allocation failed (clean seeds)");
             return RTR_ERR_CUDA;
         }
-        k_seed_keys<<<gm, kBlock, 0, s>>>(g->fwd, g->esrc, is_seed, spos, m, root, sbits, keys);
-        uint64_t* sorted = radix_sort_u64(keys, alt, ns, sbits + bits_for((uint64_t)n), rtmp, s);
+        k_seed_keys<<<gm, kBlock, 0, s>>>(g->fwd, g->esrc, is_seed, spos, m, root, rbits, keys);
+        uint64_t* sorted = radix_sort_u64(keys, alt, ns, rbits + bits_for((uint64_t)n), rtmp, s);
         const int gs = grid_for(ns, kBlock);
-        k_unit_heads<<<gs, kBlock, 0, s>>>(sorted, ns, sbits, head);
+        k_unit_heads<<<gs, kBlock, 0, s>>>(sorted, ns, rbits, head);
         exclusive_scan_u32(head, hpos, ns, d_ns + 1, htmp, s);
-        g->launches += 3 + 3 * ((sbits + bits_for((uint64_t)n) + 7) / 8);
+        k_seed_info<<<gs, kBlock, 0, s>>>(sorted, ns, rmask, g->fwd, g->esrc, g->nbors, g->deg, rec, seeds);
+        g->launches += 4 + 3 * ((rbits + bits_for((uint64_t)n) + 7) / 8);
         uint32_t nu = 0;
         RTR_CUDA_TRY(cudaMemcpyAsync(&nu, d_ns + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         RTR_CUDA_TRY(cudaStreamSynchronize(s));
@@ -409,7 +525,7 @@ int initial_clean(rtr_graph* g, double eps)
             set_error("device allocation failed (clean units)");
             return RTR_ERR_CUDA;
         }
-        k_unit_desc<<<gs, kBlock, 0, s>>>(sorted, ns, sbits, head, hpos, ecount, units, cap);
+        k_unit_desc<<<gs, kBlock, 0, s>>>(sorted, ns, rbits, head, hpos, ecount, units, cap);
         exclusive_scan_i64(cap, capoff, nu, d_cap_total, ctmp, s);
         k_unit_finish<<<grid_for(nu, kBlock), kBlock, 0, s>>>(units, cap, capoff, nu, ns, okeys);
         uint64_t* order = radix_sort_u64(okeys, oalt, nu, 64, otmp, s);
@@ -423,25 +539,25 @@ int initial_clean(rtr_graph* g, double eps)
             set_error("device allocation failed (clean stacks)");
             return RTR_ERR_CUDA;
         }
-        CleanArgs ca{g->offsets, g->nbors, g->esrc, g->deg, g->tl_off, g->tl, g->pe, g->pv, g->sup, g->st, eps,
-                     1 / (double)n};
-        const uint64_t slot_mask = (1ull << sbits) - 1;
-        // one warp per unit, persistent over the unit list
-        const int warps_per_block = kBlock / 32;
-        int blocks = (int)std::min<int64_t>((nu + warps_per_block - 1) / warps_per_block,
-                                            (int64_t)grid_for(1 << 30, kBlock, 8));
+        CleanArgs ca{g->tl, rec, g->pv, 1 / (double)n, seeds};
+        // one warp per unit, persistent over the unit list (largest units first)
+        int blocks = (int)std::min<int64_t>((nu + kCleanWarps - 1) / kCleanWarps,
+                                            (int64_t)grid_for(1 << 30, kCleanBlock, 8));
         blocks = std::max(blocks, 1);
         ktime_begin(g, KT_CLEAN_UNITS);
-        k_clean_units<<<blocks, kBlock, 0, s>>>(ca, sorted, slot_mask, units, order, nu, stacks, next_unit,
-                                                (unsigned*)(g->ctr + 1), g->ctr, g->ctr + 2);
+        k_clean_units<<<blocks, kCleanBlock, 0, s>>>(ca, units, order, nu, stacks, next_unit,
+                                                     (unsigned*)(g->ctr + 1), g->ctr, g->ctr + 2);
         ktime_end(g, KT_CLEAN_UNITS);
         g->launches += 1;
         RTR_CUDA_TRY(cudaGetLastError());
     }
+    k_clean_finish<<<gm, kBlock, 0, s>>>(g->fwd, m, rec, g->pe, g->sup, g->st);
+    g->launches += 1;
+    RTR_CUDA_TRY(cudaGetLastError());
     cudaEventRecord(e1, s);
     RTR_CUDA_TRY(cudaEventSynchronize(e1));
     cudaEventElapsedTime(&g->ms_clean, e0, e1);
-    if (g->kms[KT_CLEAN_UNITS] >= 0) ktime_read(g, KT_CLEAN_UNITS);
+    ktime_read(g, KT_CLEAN_UNITS);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     unsigned long long h[3];

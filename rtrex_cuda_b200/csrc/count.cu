@@ -116,11 +116,13 @@ __global__ void __launch_bounds__(kBlock)
 __global__ void __launch_bounds__(kBlock)
     k_tri_fill(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, const int32_t* __restrict__ fwd,
-               int64_t m, const int64_t* __restrict__ tl_off, TriEntry* __restrict__ tl)
+               const int32_t* __restrict__ frank, int64_t m, const int64_t* __restrict__ tl_off,
+               TriEntry* __restrict__ tl)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = fwd[k];
         const int32_t u = esrc[i], v = nb[i];
+        const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
         int64_t w = tl_off[i];
         intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], [&](int32_t z, int64_t pu, int64_t pv) {
             TriEntry t;
@@ -128,6 +130,9 @@ __global__ void __launch_bounds__(kBlock)
             t.eaz = (u < z) ? (int32_t)pu : partner[pu];
             t.ebz = (v < z) ? (int32_t)pv : partner[pv];
             t.dz = deg[z];
+            t.wgt = 1.0 / (double)(duv * (int64_t)t.dz);
+            t.raz = frank[t.eaz];
+            t.rbz = frank[t.ebz];
             tl[w++] = t;
         });
     }
@@ -139,7 +144,6 @@ __global__ void __launch_bounds__(kBlock)
                   const TriEntry* __restrict__ tl, double* __restrict__ pv)
 {
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t dx = deg[x];
         double acc = 0.0;
         for (int64_t i = off[x]; i < off[x + 1]; ++i) {
             const int32_t y = nb[i];
@@ -154,8 +158,8 @@ __global__ void __launch_bounds__(kBlock)
                 if (tl[mid].z <= y) a = mid + 1;
                 else b = mid;
             }
-            const int64_t dxy = dx * (int64_t)deg[y];
-            for (int64_t p = a; p < hi; ++p) acc += 1.0 / (double)(dxy * (int64_t)tl[p].dz);
+            // the entry's weight is the same integer product's reciprocal
+            for (int64_t p = a; p < hi; ++p) acc += tl[p].wgt;
         }
         pv[x] = acc;
     }
@@ -217,7 +221,8 @@ int count_triangles(rtr_graph* g)
     }
     g->tl_len = tl_len;
     ktime_begin(g, KT_TRI_FILL);
-    k_tri_fill<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd, m, g->tl_off, g->tl);
+    k_tri_fill<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd, g->frank, m,
+                                     g->tl_off, g->tl);
     ktime_end(g, KT_TRI_FILL);
     ktime_begin(g, KT_VERTEX_FOLD);
     k_vertex_fold<<<grid_for(n, kBlock), kBlock, 0, s>>>(g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl,

@@ -246,7 +246,6 @@ __device__ void delete_and_clean_seq(const ExtractArgs& a, DelEntry* stack, int6
         const int64_t dhigh = lo_is_u ? dv : du;
         const bool lower_is_a = lower == a.esrc[e];
         double acc_e = a.pe[e], acc_u = a.pv[u], acc_v = a.pv[v];
-        const int64_t duv = du * dv;
         uint32_t rem = 0;
         for (int64_t p = a.tl_off[e]; p < a.tl_off[e + 1]; ++p) {
             const TriEntry t = a.tl[p];
@@ -254,7 +253,7 @@ __device__ void delete_and_clean_seq(const ExtractArgs& a, DelEntry* stack, int6
             const int32_t ehw = lower_is_a ? t.ebz : t.eaz;
             const uint8_t slw = a.st[elw], shw = a.st[ehw];
             if (slw == ST_N || shw == ST_N) continue;
-            const double wgt = 1 / (double)(duv * (int64_t)t.dz);
+            const double wgt = t.wgt;
             acc_e -= wgt;
             const double x1 = a.pe[elw] - wgt;
             const double x2 = a.pe[ehw] - wgt;
@@ -327,9 +326,16 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
                                                             const uint64_t* __restrict__ order, int64_t nc,
                                                             unsigned* __restrict__ next_comp)
 {
+    // One warp per component: lane 0 replays the seed loop.  (Giving each
+    // thread its own component would put the largest components, which are
+    // handed out first, into the same warp and serialise them by divergence.)
+    const int lane = threadIdx.x & 31;
     while (true) {
-        const unsigned ci = atomicAdd(next_comp, 1u);
+        unsigned ci = 0;
+        if (lane == 0) ci = atomicAdd(next_comp, 1u);
+        ci = __shfl_sync(0xffffffffu, ci, 0);
         if ((int64_t)ci >= nc) return;
+        if (lane != 0) continue;
         const int64_t c = (int64_t)(uint32_t)order[ci];
         const CompDesc cd = comps[c];
         const int64_t vb = cd.vbegin, nv = cd.vcount;
@@ -665,7 +671,8 @@ int extract_clusters(rtr_graph* g)
     RTR_CUDA_TRY(cudaMemsetAsync(next_comp, 0, sizeof(unsigned) * 2, s));
     {
         const int blk = 128;
-        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nc + blk - 1) / blk, grid_for(1 << 30, blk, 16)));
+        const int64_t warps = (nc + 0);  // one component per warp
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((warps + 3) / 4, grid_for(1 << 30, blk, 16)));
         ktime_begin(g, KT_EXTRACT);
         k_extract_components<<<blocks, blk, 0, s>>>(a, comps, order, nc, next_comp);
         ktime_end(g, KT_EXTRACT);

@@ -172,10 +172,12 @@ __global__ void k_fwd_flags(const int32_t* __restrict__ esrc, const int32_t* __r
 }
 
 __global__ void k_fwd_list(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos, int64_t m2,
-                           int32_t* __restrict__ fwd)
+                           int32_t* __restrict__ fwd, int32_t* __restrict__ frank)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m2; i += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m2; i += (int64_t)gridDim.x * blockDim.x) {
+        frank[i] = flag[i] ? (int32_t)pos[i] : -1;
         if (flag[i]) fwd[pos[i]] = (int32_t)i;
+    }
 }
 
 // Host CSR path: widen-check the int64 neighbour ids, derive esrc, check order.
@@ -202,7 +204,8 @@ int finish_csr(rtr_graph* g, unsigned long long* h_ctr)
     g->deg = (int32_t*)dev_alloc(g, sizeof(int32_t) * (n + 1));
     g->partner = (int32_t*)dev_alloc(g, sizeof(int32_t) * (m2 + 1));
     g->fwd = (int32_t*)dev_alloc(g, sizeof(int32_t) * (m2 / 2 + 1));
-    if (!g->deg || !g->partner || !g->fwd) {
+    g->frank = (int32_t*)dev_alloc(g, sizeof(int32_t) * (m2 + 1));
+    if (!g->deg || !g->partner || !g->fwd || !g->frank) {
         set_error("device allocation failed for the CSR (n=%lld, 2m=%lld)", (long long)n, (long long)m2);
         return RTR_ERR_CUDA;
     }
@@ -220,7 +223,7 @@ int finish_csr(rtr_graph* g, unsigned long long* h_ctr)
     }
     k_fwd_flags<<<grid_for(m2, kBlock), kBlock, 0, s>>>(g->esrc, g->nbors, m2, flag);
     exclusive_scan_u32(flag, pos, m2, nullptr, tmp, s);
-    k_fwd_list<<<grid_for(m2, kBlock), kBlock, 0, s>>>(flag, pos, m2, g->fwd);
+    k_fwd_list<<<grid_for(m2, kBlock), kBlock, 0, s>>>(flag, pos, m2, g->fwd, g->frank);
     g->launches += 5;
     RTR_CUDA_TRY(cudaGetLastError());
     RTR_CUDA_TRY(cudaMemcpyAsync(h_ctr, g->ctr, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));

@@ -14,8 +14,9 @@
 //   sup      u32   [2m]    live triangle count
 //   st       u8    [2m]    'Y' / 'S' / 'N'
 //   pv       f64   [n]     per-vertex triangle weight
-// Triangle lists (per forward slot e=(a,b), a<b): entries {z, fwd(a,z), fwd(b,z), deg z}
-// for every common neighbour z, ascending in z.
+//   frank    int32 [2m]    forward rank of a forward slot (position in the forward list)
+// Triangle lists (per forward slot e=(a,b), a<b): one TriEntry per common
+// neighbour z, ascending in z.
 #pragma once
 
 #include <cstdint>
@@ -32,13 +33,33 @@ constexpr uint8_t ST_Y = 'Y';
 constexpr uint8_t ST_S = 'S';
 constexpr uint8_t ST_N = 'N';
 
-struct TriEntry {
+// One triangle (a, b, z) in the list of its edge (a, b), a < b.
+struct alignas(16) TriEntry {
     int32_t z;    // third vertex
-    int32_t eaz;  // forward slot of edge (a,z), a = smaller endpoint of the owner edge
+    int32_t eaz;  // forward slot of edge (a,z)
     int32_t ebz;  // forward slot of edge (b,z)
     int32_t dz;   // degree of z
+    double wgt;   // triangle weight 1/double(da*db*dz)  (Decomposition.h:97)
+    int32_t raz;  // forward rank of edge (a,z)
+    int32_t rbz;  // forward rank of edge (b,z)
 };
-static_assert(sizeof(TriEntry) == 16, "TriEntry must be one 16-byte vector");
+static_assert(sizeof(TriEntry) == 32, "TriEntry must be two 16-byte vectors");
+
+// Clean-time state of one undirected edge, indexed by forward rank: everything
+// a pop reads or writes for the edge in one 32-byte record.
+struct alignas(16) EdgeRec {
+    double pe;     // perEdge
+    double thr;    // eps * 1/double(du*dv): the edge's cleaning threshold
+    int64_t t0;    // triangle-list start
+    uint32_t cnt;  // triangle-list length
+    uint32_t ss;   // live support (low 30 bits) | status code (top 2 bits)
+};
+static_assert(sizeof(EdgeRec) == 32, "EdgeRec is 32 bytes");
+constexpr uint32_t SS_SUP = (1u << 30) - 1u;
+constexpr uint32_t SS_Y = 0u;
+constexpr uint32_t SS_S = 1u << 30;
+constexpr uint32_t SS_N = 2u << 30;
+constexpr uint32_t SS_CODE = 3u << 30;
 
 // Error codes returned through the C ABI are the rtr_status values of rtr.h.
 

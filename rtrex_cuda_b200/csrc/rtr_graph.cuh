@@ -24,7 +24,8 @@ struct rtr_graph {
     int32_t* esrc = nullptr;
     int32_t* partner = nullptr;
     int32_t* deg = nullptr;
-    int32_t* fwd = nullptr;  // the m forward slots, ascending
+    int32_t* fwd = nullptr;    // the m forward slots, ascending
+    int32_t* frank = nullptr;  // [2m] position of a forward slot in fwd
 
     // weighted-triangle state
     double* pe = nullptr;
