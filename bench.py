@@ -141,6 +141,24 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ replicas
+
+def replica_max(x: float, world: int, device) -> float:
+    """Max of a per-rank time over all ranks (the slowest replica bounds the step)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(edges_per_rank: int, world: int, ms_step: float) -> float:
+    """Whole-job edges/s: every rank decomposes its own copy in ms_step (max over ranks)."""
+    return world * edges_per_rank / (ms_step / 1e3)
+
+
 # ------------------------------------------------------------------ GPU leg
 
 class ClockSampler:
@@ -253,11 +271,7 @@ def ours_arm(args):
             dist.barrier()
 
     def allmax(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(x, world, torch.device("cuda", dev))
 
     n, u, v = workload()
     m = int(u.size)
@@ -288,7 +302,7 @@ def ours_arm(args):
     barrier()
     launches = g.stats()["launches"] - launches0
     ms_step = allmax(float(np.mean(step_ms)))
-    value = world * m / (ms_step / 1e3)
+    value = replica_value(m, world, ms_step)
 
     # roofline of the dominant kernel (per-launch averages over the timed steps)
     names = ["k_edge_fold", "k_tri_fill", "k_vertex_fold", "k_clean_units", "k_extract_components"]

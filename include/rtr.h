@@ -44,7 +44,9 @@ enum rtr_status {
 };
 
 enum rtr_flags {
-    RTR_FLAG_SIMPLIFY = 1 /* drop self-loops and duplicate pairs instead of rejecting them */
+    RTR_FLAG_SIMPLIFY = 1,     /* drop self-loops and duplicate pairs instead of rejecting them */
+    RTR_FLAG_RTREX_OUTPUTS = 2 /* rtr_run_file also writes what the sequential RTRex CLI writes besides the
+                                  decomposition: connected-components-<name>-* and amazon_cleaned_edges.txt */
 };
 
 /* Library version string and the calling thread's last error message. */
@@ -125,6 +127,21 @@ int rtr_get_cluster_of(const rtr_graph* g, int64_t* cluster_of);
  * kernel launches issued for this graph so far; diagnostic counter of the
  * reference's residual self-check (Decomposition.h:273-277). */
 int rtr_get_stats(const rtr_graph* g, double* ms4, int64_t* launches, int64_t* residual_warnings);
+
+/* Connected components of the original graph, in creation order (ascending
+ * smallest vertex), each listing its vertices in breadth-first discovery order.
+ * Replaces: connectedComp (RTRex_Sequential/Escape/Decomposition.h:1023-1068). */
+int rtr_connected_components(rtr_graph* g, int64_t* n_components);
+
+/* Copy the components: component k has vertices vert[off[k] .. off[k+1]) in
+ * discovery order.  Sizes: off[n_components+1], vert[n]. */
+int rtr_get_components(const rtr_graph* g, int64_t* off, int64_t* vert);
+
+/* Write <name>-decomposition.txt / -stats.txt / -freq.txt / -cut.txt for the
+ * connected components, as RTRex.cpp:203-204 prints them through
+ * printDecomposition (members in the order the reference's unordered_set
+ * iterates them after inserting them in discovery order). */
+int rtr_write_components(const rtr_graph* g, const char* name);
 
 /* Device times (ms, CUDA events on the graph's stream) of the last run of the
  * main kernels: ms[0] edge fold, [1] triangle-list fill, [2] vertex fold,

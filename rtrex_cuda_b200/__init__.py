@@ -81,6 +81,9 @@ def lib():
     L.rtr_get_clusters.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.rtr_get_cluster_of.argtypes = [_vp, _vp]
     L.rtr_num_clusters.argtypes = [_vp, P(_i64)]
+    L.rtr_connected_components.argtypes = [_vp, P(_i64)]
+    L.rtr_get_components.argtypes = [_vp, _vp, _vp]
+    L.rtr_write_components.argtypes = [_vp, ctypes.c_char_p]
     L.rtr_get_stats.argtypes = [_vp, _vp, P(_i64), P(_i64)]
     L.rtr_get_kernel_ms.argtypes = [_vp, _vp, ctypes.c_int]
     L.rtr_write_decomposition.argtypes = [_vp, ctypes.c_char_p]

@@ -321,9 +321,14 @@ int rtr_get_weights(const rtr_graph* gc, double* perEdge, double* perVertex, uin
 int rtr_get_status(const rtr_graph* gc, uint8_t* status)
 {
     rtr_graph* g = const_cast<rtr_graph*>(gc);
-    if (!g || g->stage < 3 || !status) {
+    if (!g || g->stage < 3) {
         set_error("status is not available before the clean");
         return RTR_ERR_STATE;
+    }
+    if (g->m2 == 0) return RTR_OK;
+    if (!status) {
+        set_error("null status buffer");
+        return RTR_ERR_ARG;
     }
     RTR_CUDA_TRY(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
@@ -386,6 +391,36 @@ int rtr_get_cluster_of(const rtr_graph* gc, int64_t* cluster_of)
     }
     RTR_CUDA_TRY(cudaSetDevice(g->device));
     return copy_i32_as_i64(g, g->cluster_of, g->n, cluster_of);
+}
+
+int rtr_connected_components(rtr_graph* g, int64_t* ncomp)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    const int rc = connected_components(g);
+    if (rc) return rc;
+    if (ncomp) *ncomp = g->ncc;
+    return RTR_OK;
+}
+
+int rtr_get_components(const rtr_graph* gc, int64_t* off, int64_t* vert)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || !g->cc_vert) {
+        set_error("components are not computed yet");
+        return RTR_ERR_STATE;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    if (off) {
+        RTR_CUDA_TRY(cudaMemcpyAsync(off, g->cc_off, sizeof(int64_t) * (g->ncc + 1), cudaMemcpyDeviceToHost,
+                                     g->stream));
+        RTR_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    if (vert) return copy_i32_as_i64(g, g->cc_vert, g->n, vert);
+    return RTR_OK;
 }
 
 int rtr_get_stats(const rtr_graph* g, double* ms4, int64_t* launches, int64_t* residual)

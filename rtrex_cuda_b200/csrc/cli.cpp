@@ -5,7 +5,9 @@
 // Same positional arguments and outputs as RTRex_CUDA (RTRex_CUDA/main.cu:343-391):
 // writes <P><output_name>-{decomposition,stats,freq,cut}.txt with P defaulting
 // to "RTRex-CUDA-"; pass --prefix RTRex- for the sequential RTRex driver's names
-// (RTRex_Sequential/clustering/RTRex.cpp:194).  Exit code 1 on any failure,
+// (RTRex_Sequential/clustering/RTRex.cpp:194); with that prefix the CLI also
+// writes the RTRex driver's connected-components-<name>-* files and the
+// amazon_cleaned_edges.txt survivor dump (RTRex.cpp:203-204, Decomposition.h:441-452).  Exit code 1 on any failure,
 // as the reference exits 1 when the graph cannot be loaded.
 #include "../../include/rtr.h"
 
@@ -23,6 +25,7 @@ int main(int argc, char** argv)
     for (int i = 1; i < argc; ++i) {
         if (!strcmp(argv[i], "--prefix") && i + 1 < argc) {
             prefix = argv[++i];
+            if (prefix == "RTRex-") flags |= RTR_FLAG_RTREX_OUTPUTS;
         } else if (!strcmp(argv[i], "--simplify")) {
             flags |= RTR_FLAG_SIMPLIFY;
         } else if (npos < 4) {

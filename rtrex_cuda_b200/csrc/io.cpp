@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 namespace rtr {
@@ -140,23 +141,11 @@ int rtr_load_escape(const char* path, int64_t* n_out, int64_t* m_out, int64_t** 
 // are ranked with std::sort on the size comparator from creation order, as the
 // reference does, so equal-size clusters land in the same lines; members are
 // written in the reference's set-iteration order.
-int rtr_write_decomposition(const rtr_graph* g, const char* name_c)
+static int write_clusters(const char* name_c, int64_t n, const std::vector<int64_t>& off,
+                          const std::vector<int64_t>& nb, int64_t k, const std::vector<int64_t>& nv,
+                          const std::vector<int64_t>& ne, const std::vector<int64_t>& coff,
+                          const std::vector<int64_t>& vert, const std::vector<int64_t>& cluster_of)
 {
-    if (!g || !name_c) {
-        rtr::set_error("null argument");
-        return RTR_ERR_ARG;
-    }
-    int64_t n = 0, m = 0, k = 0;
-    int rc = rtr_graph_info(g, &n, &m);
-    if (rc) return rc;
-    std::vector<int64_t> off(n + 1), nb(2 * m), cluster_of(n);
-    if ((rc = rtr_get_csr(g, off.data(), nb.data()))) return rc;
-    if ((rc = rtr_get_cluster_of(g, cluster_of.data()))) return rc;
-    if ((rc = rtr_num_clusters(g, &k))) return rc;
-    std::vector<int64_t> seed(k), nv(k), ne(k), cut(k), coff(k + 1), vert(n);
-    if ((rc = rtr_get_clusters(g, seed.data(), nv.data(), ne.data(), cut.data(), coff.data(), vert.data())))
-        return rc;
-
     const std::string name(name_c);
     printf("\n--------------------------------------------\n");
     printf("Generating details of %s decomposition\n", name.c_str());
@@ -218,6 +207,90 @@ int rtr_write_decomposition(const rtr_graph* g, const char* name_c)
     return RTR_OK;
 }
 
+int rtr_write_decomposition(const rtr_graph* g, const char* name_c)
+{
+    if (!g || !name_c) {
+        rtr::set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    int64_t n = 0, m = 0, k = 0;
+    int rc = rtr_graph_info(g, &n, &m);
+    if (rc) return rc;
+    std::vector<int64_t> off(n + 1), nb(2 * m), cluster_of(n);
+    if ((rc = rtr_get_csr(g, off.data(), nb.data()))) return rc;
+    if ((rc = rtr_get_cluster_of(g, cluster_of.data()))) return rc;
+    if ((rc = rtr_num_clusters(g, &k))) return rc;
+    std::vector<int64_t> seed(k), nv(k), ne(k), cut(k), coff(k + 1), vert(n);
+    if ((rc = rtr_get_clusters(g, seed.data(), nv.data(), ne.data(), cut.data(), coff.data(), vert.data())))
+        return rc;
+    return write_clusters(name_c, n, off, nb, k, nv, ne, coff, vert, cluster_of);
+}
+
+// The components' member order: the reference inserts a component's vertices
+// into an unordered_set in discovery order (Decomposition.h:1038-1056) and
+// prints them in that set's iteration order, so the writer replays the inserts.
+int rtr_write_components(const rtr_graph* g, const char* name_c)
+{
+    if (!g || !name_c) {
+        rtr::set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    int64_t n = 0, m = 0;
+    int rc = rtr_graph_info(g, &n, &m);
+    if (rc) return rc;
+    std::vector<int64_t> off(n + 1), nb(2 * m), disc(n);
+    if ((rc = rtr_get_csr(g, off.data(), nb.data()))) return rc;
+    int64_t k = 0;
+    {
+        // number of components = entries of the offsets array minus one
+        std::vector<int64_t> tmp(n + 2, -1);
+        if ((rc = rtr_get_components(g, tmp.data(), disc.data()))) return rc;
+        while (k < n && tmp[k + 1] > tmp[k]) ++k;
+        std::vector<int64_t> coff(tmp.begin(), tmp.begin() + k + 1);
+        std::vector<int64_t> nv(k), ne(k), vert(n), cluster_of(n);
+        int64_t w = 0;
+        for (int64_t c = 0; c < k; ++c) {
+            std::unordered_set<int64_t> members;
+            for (int64_t p = coff[c]; p < coff[c + 1]; ++p) members.insert(disc[p]);
+            int64_t deg_sum = 0;
+            const int64_t start = w;
+            for (int64_t v : members) {
+                vert[w++] = v;
+                cluster_of[v] = c;
+                deg_sum += off[v + 1] - off[v];
+            }
+            nv[c] = w - start;
+            ne[c] = deg_sum / 2;  // populateStats: every neighbour of a component member is inside it
+        }
+        return write_clusters(name_c, n, off, nb, k, nv, ne, coff, vert, cluster_of);
+    }
+}
+
+// The survivor dump initialClean writes into the working directory
+// (Decomposition.h:416-455): the 'Y' edges u<v, sorted.
+static int write_cleaned_edges(const rtr_graph* g)
+{
+    int64_t n = 0, m = 0;
+    int rc = rtr_graph_info(g, &n, &m);
+    if (rc) return rc;
+    std::vector<int64_t> off(n + 1), nb(2 * m + 1);
+    std::vector<uint8_t> st(2 * m + 1);
+    if ((rc = rtr_get_csr(g, off.data(), nb.data()))) return rc;
+    if ((rc = rtr_get_status(g, st.data()))) return rc;
+    int64_t remaining = 0;
+    FILE* f = fopen("amazon_cleaned_edges.txt", "w");
+    for (int64_t u = 0; u < n; ++u)
+        for (int64_t j = off[u]; j < off[u + 1]; ++j)
+            if (st[j] == 'Y') {
+                ++remaining;
+                if (f && u < nb[j]) fprintf(f, "%" PRId64 " %" PRId64 "\n", u, nb[j]);
+            }
+    if (f) fclose(f);
+    printf("Edges remaining after initialClean (Directed): %" PRId64 "\n", remaining);
+    printf("Edges remaining after initialClean (Undirected): %" PRId64 "\n", remaining / 2);
+    return RTR_OK;
+}
+
 int rtr_run_file(const char* graph_path, const char* name, double eps, int device, const char* prefix, int flags)
 {
     if (!graph_path || !name) {
@@ -239,7 +312,8 @@ int rtr_run_file(const char* graph_path, const char* name, double eps, int devic
         printf("Total triangles = %" PRId64 "\n", total);
         if (!(rc = rtr_clean(g, eps, &left))) {
             printf("Total triangle count, post cleaning = %" PRId64 "\n", left);
-            rc = rtr_extract(g, &ncl);
+            if (flags & RTR_FLAG_RTREX_OUTPUTS) rc = write_cleaned_edges(g);
+            if (!rc) rc = rtr_extract(g, &ncl);
         }
     }
     if (!rc) {
@@ -250,6 +324,11 @@ int rtr_run_file(const char* graph_path, const char* name, double eps, int devic
         printf("Time for getting the clusters: %gs \n", ms[3] / 1e3);
         printf("Total clusters extracted: %" PRId64 "\n", ncl);
         rc = rtr_write_decomposition(g, (std::string(prefix ? prefix : "") + name).c_str());
+    }
+    if (!rc && (flags & RTR_FLAG_RTREX_OUTPUTS)) {
+        int64_t ncomp = 0;
+        rc = rtr_connected_components(g, &ncomp);
+        if (!rc) rc = rtr_write_components(g, (std::string("connected-components-") + name).c_str());
     }
     rtr_graph_destroy(g);
     return rc;

@@ -48,6 +48,11 @@ struct rtr_graph {
     int64_t* cl_cut = nullptr;     // [ncl] cut edges
     int32_t* cluster_of = nullptr; // [n]
 
+    // connected components of the original graph, creation order, BFS discovery order inside
+    int64_t ncc = 0;
+    int64_t* cc_off = nullptr;   // [ncc+1]
+    int32_t* cc_vert = nullptr;  // [n]
+
     double eps = 0.3;
     int stage = 0;  // 1 built, 2 counted, 3 cleaned, 4 extracted
 
@@ -97,5 +102,6 @@ int build_csr_from_host_csr(rtr_graph* g, const int64_t* h_offsets, const int64_
 int count_triangles(rtr_graph* g);
 int initial_clean(rtr_graph* g, double eps);
 int extract_clusters(rtr_graph* g);
+int connected_components(rtr_graph* g);
 
 }  // namespace rtr

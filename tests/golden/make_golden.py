@@ -8,8 +8,9 @@ graph and records, per stage, the reference's results:
 * clean:   triangles left, sha256 of the status bytes, perEdge bits, perVertex bits
 * extract: number of clusters and sha256 of the cluster list (creation order,
            "nv ne cut : members" in set-iteration order, one line per cluster)
-* files:   sha256 of RTRex-<name>-{decomposition,stats,freq,cut}.txt written by
-           the reference CLI (oracle/_ref/RTRex <graph> <name> <eps> s)
+* files:   sha256 of RTRex-<name>-{decomposition,stats,freq,cut}.txt, of
+           connected-components-<name>-*.txt (cc_*) and of amazon_cleaned_edges.txt
+           written by the reference CLI (oracle/_ref/RTRex <graph> <name> <eps> s)
 
 small_test (the reference's RTRex_Sequential/Example/small-test.txt graph)
 additionally stores full arrays in small_test.npz.  Graph inputs are either
@@ -80,8 +81,12 @@ def run_reference_cli(cli_bin: str, path: str, eps: float):
     with tempfile.TemporaryDirectory() as td:
         subprocess.run([cli_bin, path, "g", repr(eps), "s"], check=True, cwd=td, stdout=subprocess.DEVNULL,
                        stderr=subprocess.DEVNULL)
-        return {kind: sha(open(os.path.join(td, f"RTRex-g-{kind}.txt"), "rb").read())
-                for kind in ("decomposition", "stats", "freq", "cut")}
+        out = {kind: sha(open(os.path.join(td, f"RTRex-g-{kind}.txt"), "rb").read())
+               for kind in ("decomposition", "stats", "freq", "cut")}
+        for kind in ("decomposition", "stats", "freq", "cut"):
+            out["cc_" + kind] = sha(open(os.path.join(td, f"connected-components-g-{kind}.txt"), "rb").read())
+        out["cleaned_edges"] = sha(open(os.path.join(td, "amazon_cleaned_edges.txt"), "rb").read())
+        return out
 
 
 def main():
