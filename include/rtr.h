@@ -68,6 +68,21 @@ int rtr_graph_create_from_edges(const int64_t* src, const int64_t* dst, int64_t 
  *           (RTRex_CUDA/gpu_graph.cuh:47-52) with allocateDeviceState (:57). */
 int rtr_graph_create_from_csr(const int64_t* offsets, const int64_t* nbors, int64_t n, int device, rtr_graph** out);
 
+/* Build ONE device graph that holds K independent graphs (their disjoint
+ * union) so a single rtr_decompose runs them all: graph k has nverts[k]
+ * vertices and the undirected pairs (src[i], dst[i]), i in [eoff[k], eoff[k+1]),
+ * in graph-local ids.  Graph k's vertex v becomes union vertex base_k + v with
+ * base_k = nverts[0] + ... + nverts[k-1]; clusters, weights and statuses come
+ * back in union ids and equal, graph by graph, what a separate decomposition of
+ * each graph returns (the extraction hashes graph-local ids, so set-iteration
+ * orders match).  No counterpart in the reference, which decomposes one graph
+ * per process. */
+int rtr_batch_create(const int64_t* src, const int64_t* dst, const int64_t* eoff, const int64_t* nverts, int64_t K,
+                     int device, int flags, rtr_graph** out);
+
+/* Clusters per graph of a batch after extraction (counts[K]). */
+int rtr_batch_cluster_counts(const rtr_graph* g, int64_t* counts);
+
 /* Release every device buffer of the graph.
  * Replaces: freeDeviceGraph (RTRex_CUDA/gpu_graph.cuh:62). */
 int rtr_graph_destroy(rtr_graph* g);

@@ -81,6 +81,8 @@ def lib():
     L.rtr_get_clusters.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.rtr_get_cluster_of.argtypes = [_vp, _vp]
     L.rtr_num_clusters.argtypes = [_vp, P(_i64)]
+    L.rtr_batch_create.argtypes = [_vp, _vp, _vp, _vp, _i64, ctypes.c_int, ctypes.c_int, P(_vp)]
+    L.rtr_batch_cluster_counts.argtypes = [_vp, _vp]
     L.rtr_connected_components.argtypes = [_vp, P(_i64)]
     L.rtr_get_components.argtypes = [_vp, _vp, _vp]
     L.rtr_write_components.argtypes = [_vp, ctypes.c_char_p]
@@ -140,6 +142,27 @@ class Graph:
         _check(lib().rtr_graph_create_from_edges(_ptr(src), _ptr(dst), src.size, int(n), int(device),
                                                  RTR_FLAG_SIMPLIFY if simplify else 0, ctypes.byref(h)))
         return cls(h.value)
+
+    @classmethod
+    def batch(cls, graphs, device: int = 0, simplify: bool = False) -> "Graph":
+        """One device graph holding independent graphs [(n, src, dst), ...] (disjoint union)."""
+        nverts = np.array([int(g[0]) for g in graphs], dtype=np.int64)
+        eoff = np.zeros(len(graphs) + 1, dtype=np.int64)
+        eoff[1:] = np.cumsum([len(g[1]) for g in graphs])
+        src = np.ascontiguousarray(np.concatenate([np.asarray(g[1], np.int64) for g in graphs]))
+        dst = np.ascontiguousarray(np.concatenate([np.asarray(g[2], np.int64) for g in graphs]))
+        h = ctypes.c_void_p()
+        _check(lib().rtr_batch_create(_ptr(src), _ptr(dst), _ptr(eoff), _ptr(nverts), len(graphs), int(device),
+                                      RTR_FLAG_SIMPLIFY if simplify else 0, ctypes.byref(h)))
+        out = cls(h.value)
+        out.vertex_bases = np.concatenate([[0], np.cumsum(nverts)])
+        return out
+
+    def batch_cluster_counts(self) -> np.ndarray:
+        k = len(self.vertex_bases) - 1
+        out = np.zeros(k, np.int64)
+        _check(lib().rtr_batch_cluster_counts(self._h, _ptr(out)))
+        return out
 
     @classmethod
     def from_csr(cls, offsets, nbors, device: int = 0) -> "Graph":

@@ -29,6 +29,20 @@ __global__ void k_expand_pe(const double* __restrict__ pe, const uint32_t* __res
     }
 }
 
+// vbase[v] = first vertex id of v's graph (binary search over the batch bases).
+__global__ void k_fill_vbase(const int64_t* __restrict__ bases, int64_t K, int64_t n, int32_t* __restrict__ vbase)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        int64_t lo = 0, hi = K;  // largest k with bases[k] <= v
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (bases[mid] <= v) lo = mid;
+            else hi = mid;
+        }
+        vbase[v] = (int32_t)bases[lo];
+    }
+}
+
 __global__ void k_widen32(const int32_t* __restrict__ in, int64_t* __restrict__ out, int64_t k)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x)
@@ -149,6 +163,89 @@ int rtr_graph_create_from_edges(const int64_t* src, const int64_t* dst, int64_t 
     return rc;
 }
 
+int rtr_batch_create(const int64_t* src, const int64_t* dst, const int64_t* eoff, const int64_t* nverts, int64_t K,
+                     int device, int flags, rtr_graph** out)
+{
+    if (!eoff || !nverts || K <= 0 || ((!src || !dst) && eoff[K] > 0)) {
+        set_error("rtr_batch_create: null arrays or empty batch");
+        return RTR_ERR_ARG;
+    }
+    std::vector<int64_t> bases(K + 1, 0);
+    for (int64_t k = 0; k < K; ++k) {
+        if (nverts[k] <= 0 || eoff[k + 1] < eoff[k]) {
+            set_error("rtr_batch_create: graph %lld has no vertices or a negative edge range", (long long)k);
+            return RTR_ERR_INPUT;
+        }
+        bases[k + 1] = bases[k] + nverts[k];
+    }
+    const int64_t n = bases[K], m = eoff[K];
+    if (n >= (int64_t)INT32_MAX) {
+        set_error("rtr_batch_create: %lld vertices in total exceeds the int32 id width", (long long)n);
+        return RTR_ERR_LIMIT;
+    }
+    // union edge list with graph-local ids shifted by each graph's base
+    std::vector<int64_t> gs((size_t)m), gd((size_t)m);
+    for (int64_t k = 0; k < K; ++k)
+        for (int64_t i = eoff[k]; i < eoff[k + 1]; ++i) {
+            if (src[i] < 0 || src[i] >= nverts[k] || dst[i] < 0 || dst[i] >= nverts[k]) {
+                set_error("rtr_batch_create: graph %lld edge %lld has an endpoint outside [0, %lld)", (long long)k,
+                          (long long)(i - eoff[k]), (long long)nverts[k]);
+                return RTR_ERR_INPUT;
+            }
+            gs[i] = src[i] + bases[k];
+            gd[i] = dst[i] + bases[k];
+        }
+    int rc = rtr_graph_create_from_edges(gs.data(), gd.data(), m, n, device, flags, out);
+    if (rc) return rc;
+    rtr_graph* g = *out;
+    g->nbatch = K;
+    g->batch_vbase = new (std::nothrow) int64_t[K + 1];
+    Scratch sc(g);
+    int64_t* dbases = (int64_t*)sc.get(sizeof(int64_t) * (K + 1));
+    g->vbase = (int32_t*)dev_alloc(g, sizeof(int32_t) * (n + 1));
+    if (!g->batch_vbase || !dbases || !g->vbase) {
+        rtr_graph_destroy(g);
+        *out = nullptr;
+        set_error("allocation failed for the batch bases");
+        return RTR_ERR_CUDA;
+    }
+    for (int64_t k = 0; k <= K; ++k) g->batch_vbase[k] = bases[k];
+    RTR_CUDA_TRY(cudaMemcpyAsync(dbases, bases.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice, g->stream));
+    k_fill_vbase<<<grid_for(n, 256), 256, 0, g->stream>>>(dbases, K, n, g->vbase);
+    g->launches += 1;
+    RTR_CUDA_TRY(cudaGetLastError());
+    RTR_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    return RTR_OK;
+}
+
+int rtr_batch_cluster_counts(const rtr_graph* gc, int64_t* counts)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || !counts || g->nbatch <= 0) {
+        set_error("not a batch graph");
+        return RTR_ERR_ARG;
+    }
+    if (g->stage < 4) {
+        set_error("clusters are not extracted yet");
+        return RTR_ERR_STATE;
+    }
+    std::vector<int64_t> seed(g->ncl);
+    int rc = copy_i32_as_i64(g, g->cl_seed, g->ncl, seed.data());
+    if (rc) return rc;
+    for (int64_t k = 0; k < g->nbatch; ++k) counts[k] = 0;
+    for (int64_t c = 0; c < g->ncl; ++c) {
+        const int64_t* b = g->batch_vbase;
+        int64_t lo = 0, hi = g->nbatch;
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (b[mid] <= seed[c]) lo = mid;
+            else hi = mid;
+        }
+        counts[lo]++;
+    }
+    return RTR_OK;
+}
+
 int rtr_graph_create_from_csr(const int64_t* offsets, const int64_t* nbors, int64_t n, int device, rtr_graph** out)
 {
     if (!offsets || (!nbors && offsets[n] > 0)) {
@@ -184,6 +281,7 @@ int rtr_graph_destroy(rtr_graph* g)
     for (int k = 0; k < 2 * rtr_graph::kTimers; ++k)
         if (g->kev[k]) cudaEventDestroy(g->kev[k]);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+    delete[] g->batch_vbase;
     delete g;
     return RTR_OK;
 }

@@ -191,6 +191,7 @@ struct DelEntry {
 };
 
 struct ExtractArgs {
+    const int32_t* vbase;  // per-vertex id base of its graph in a batch (null: a single graph)
     const int64_t* off;
     const int32_t* nb;
     const int32_t* esrc;
@@ -349,6 +350,10 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
             a.ncl[c] = 1;
             continue;
         }
+        // The member set hashes vertex ids; in a batch the ids are offset per
+        // graph, so the set works on graph-local ids to iterate as the graph
+        // alone would.
+        const int32_t base = a.vbase ? a.vbase[a.vlist[vb]] : 0;
         int32_t* ukey = a.ukey + vb;
         int32_t* unext = a.unext + vb;
         int32_t* ubucket = a.ubucket + cd.bbase;
@@ -363,13 +368,13 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
             const int64_t du = a.deg[u];
             UsetOrder S;
             S.init(ukey, unext, ubucket);
-            S.insert(u);
+            S.insert(u - base);
             a.clustered[u] = 1;
             const int64_t r0 = a.off[u], r1 = a.off[u + 1];
             for (int64_t j = r0; j < r1; ++j) {
                 if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
                 const int32_t v = a.nb[j];
-                S.insert(v);
+                S.insert(v - base);
                 a.nbd[v] = 1;
                 a.clustered[v] = 1;
             }
@@ -433,7 +438,7 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
                 }
             }
             for (int64_t k = 0; k <= maxind; ++k) {
-                S.insert(cand[k].vertex);
+                S.insert(cand[k].vertex - base);
                 a.clustered[cand[k].vertex] = 1;
             }
             // The reference clears the bit of every neighbour of u (Decomposition.h:879-883).
@@ -450,12 +455,12 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
             a.hdr_seed[vb + ncl] = u;
             a.hdr_start[vb + ncl] = out;
             a.hdr_size[vb + ncl] = S.size;
-            for (int32_t p = S.head; p != -1; p = S.next[p]) a.out_vert[out++] = S.key[p];
+            for (int32_t p = S.head; p != -1; p = S.next[p]) a.out_vert[out++] = S.key[p] + base;
             ++ncl;
 
             int64_t top = 0;
             for (int32_t p = S.head; p != -1; p = S.next[p]) {
-                const int32_t z = S.key[p];
+                const int32_t z = S.key[p] + base;
                 for (int64_t j = a.off[z]; j < a.off[z + 1]; ++j) {
                     const int64_t f = fwd_slot(z, j, a.nb, a.partner);
                     if (a.st[f] != ST_Y) continue;
@@ -626,6 +631,7 @@ int extract_clusters(rtr_graph* g)
     RTR_CUDA_TRY(cudaStreamSynchronize(s));
 
     ExtractArgs a;
+    a.vbase = g->vbase;
     a.off = g->offsets;
     a.nb = g->nbors;
     a.esrc = g->esrc;

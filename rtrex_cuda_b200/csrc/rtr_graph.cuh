@@ -53,6 +53,11 @@ struct rtr_graph {
     int64_t* cc_off = nullptr;   // [ncc+1]
     int32_t* cc_vert = nullptr;  // [n]
 
+    // batch of independent graphs held as one disjoint union
+    int64_t nbatch = 0;
+    int32_t* vbase = nullptr;   // [n] first vertex id of the vertex's graph (null: single graph)
+    int64_t* batch_vbase = nullptr;  // host copy, [nbatch+1]
+
     double eps = 0.3;
     int stage = 0;  // 1 built, 2 counted, 3 cleaned, 4 extracted
 

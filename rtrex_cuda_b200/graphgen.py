@@ -233,3 +233,15 @@ if __name__ == "__main__":  # pragma: no cover - manual use
     g = config_graph(name)
     write_escape(out, *g)
     print(name, g[0], g[1].size, os.path.getsize(out))
+
+
+def sbm_batch(count: int, seed0: int = 4000, m_lo: float = 1e3, m_hi: float = 2e5):
+    """The batched workload: graph i is an SBM (4-64 blocks, intra-block mean
+    degree 12, inter-block mean degree 2) whose edge target is log-uniform in
+    [m_lo, m_hi], seeded with seed0 + i."""
+    out = []
+    for i in range(count):
+        rng = np.random.Generator(np.random.PCG64(seed0 + i))
+        m_target = int(np.exp(rng.uniform(np.log(m_lo), np.log(m_hi))))
+        out.append(sbm(m_target, seed0 + i))
+    return out
