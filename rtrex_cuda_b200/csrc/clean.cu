@@ -247,6 +247,22 @@ constexpr int kCleanBlock = 128;
 constexpr int kCleanWarps = kCleanBlock / 32;
 constexpr int kSmemStack = 256;  // newest stack entries of each warp live in shared memory
 
+// Shared memory of one warp.
+struct WarpSmem {
+    StackEntry stack[kSmemStack];  // cascade stack, newest entries
+    TriEntry went[32][32];         // first 32 triangles of each seed in the window
+    double sw[32];                 // per-lane triangle weights of the current chunk
+};
+
+// Asynchronous 16-byte global -> shared copy (no register round trip); all of
+// a window's copies are issued back to back and waited for once.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Per-warp cascade stack: the newest entries in shared memory, older ones
 // spilled in order to the unit's global region (LIFO order is preserved).
 struct WarpStack {
@@ -259,14 +275,16 @@ struct WarpStack {
 
 // Pop one edge: deleteAndClean's loop body (Decomposition.h:152-281) for the
 // whole warp.  Returns the number of triangles removed, or -1 on overflow.
-__device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c, WarpStack& ws, double* sw,
-                                        unsigned* err, unsigned long long* diag)
+__device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c, const TriEntry* staged, WarpStack& ws,
+                                        double* sw, unsigned* err, unsigned long long* diag)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int32_t e = c.e, u = c.first, v = c.second;
     const int32_t du = c.dfirst, dv = c.dsecond;
-    // round trip 1: the edge's record, its endpoints' weights, its first 32 triangles
+    // round trip 1: the edge's record, its endpoints' weights, its first 32
+    // triangles -- which a window seed already has in shared memory, so for a
+    // seed the second round trip below is issued together with this one.
     uint32_t s_e = 0;
     double scal = 0.0;
     if (lane == 0) s_e = a.rec[e].ss;
@@ -274,7 +292,17 @@ __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c,
     else if (lane == 2) scal = a.pv[u];
     else if (lane == 3) scal = a.pv[v];
     TriEntry t{};
-    if (lane < c.cnt) t = a.tl[c.t0 + lane];
+    if (lane < c.cnt) t = staged ? staged[lane] : a.tl[c.t0 + lane];
+    const bool lo_is_u0 = du < dv;
+    const int32_t lower0 = lo_is_u0 ? u : v;
+    const bool lower_is_a0 = lower0 == (u < v ? u : v);
+    EdgeRec q1{}, q2{};
+    double qz = 0.0;
+    if (staged && lane < c.cnt) {
+        q1 = a.rec[lower_is_a0 ? t.raz : t.rbz];
+        q2 = a.rec[lower_is_a0 ? t.rbz : t.raz];
+        qz = a.pv[t.z];
+    }
     s_e = __shfl_sync(0xffffffffu, s_e, 0) & SS_SUP;
     double acc_e = __shfl_sync(0xffffffffu, scal, 1);
     double acc_u = __shfl_sync(0xffffffffu, scal, 2);
@@ -305,9 +333,15 @@ __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c,
         r2.ss = SS_N;
         double pz = 0.0;
         if (valid) {
-            r1 = a.rec[rlw];
-            r2 = a.rec[rhw];
-            pz = a.pv[t.z];
+            if (base == 0 && staged) {
+                r1 = q1;
+                r2 = q2;
+                pz = qz;
+            } else {
+                r1 = a.rec[rlw];
+                r2 = a.rec[rhw];
+                pz = a.pv[t.z];
+            }
         }
         const uint32_t c1 = r1.ss & SS_CODE, c2 = r2.ss & SS_CODE;
         const bool live = valid && c1 != SS_N && c2 != SS_N;
@@ -372,17 +406,17 @@ __global__ void __launch_bounds__(kCleanBlock)
                   StackEntry* __restrict__ stacks, unsigned* __restrict__ next_unit, unsigned* __restrict__ err,
                   unsigned long long* __restrict__ total, unsigned long long* __restrict__ diag)
 {
-    __shared__ StackEntry s_stack[kCleanWarps][kSmemStack];
-    __shared__ double s_w[kCleanWarps][32];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double* sw = s_w[wid];
+    WarpSmem& sm = reinterpret_cast<WarpSmem*>(smem_raw)[wid];
+    double* sw = sm.sw;
     while (true) {
         unsigned ui = 0;
         if (lane == 0) ui = atomicAdd(next_unit, 1u);
         ui = __shfl_sync(0xffffffffu, ui, 0);
         if ((int64_t)ui >= nu) break;
         const UnitDesc ud = units[(uint32_t)order[ui]];
-        WarpStack ws{s_stack[wid], stacks + ud.stack_base, 0, ud.stack_cap, 0};
+        WarpStack ws{sm.stack, stacks + ud.stack_base, 0, ud.stack_cap, 0};
         int64_t sp = ud.seed_end;  // seeds [seed_begin, sp) not yet loaded
         // Window of the next 32 seeds in pop order (lane k = seed sp_at_load-1-k).
         unsigned wmask = 0;
@@ -390,6 +424,7 @@ __global__ void __launch_bounds__(kCleanBlock)
         unsigned long long removed = 0;
         while (true) {
             StackEntry cur;
+            const TriEntry* staged = nullptr;
             if (ws.scount > 0) {
                 cur = ws.sm[--ws.scount];
             } else if (ws.gtop > 0) {
@@ -417,10 +452,24 @@ __global__ void __launch_bounds__(kCleanBlock)
                     }
                     wmask = __ballot_sync(0xffffffffu, live_seed);
                     sp = lo;
+                    // stage the first 32 triangles of every live seed (static data)
+                    for (unsigned mm = wmask; mm; mm &= mm - 1) {
+                        const int k = __ffs(mm) - 1;
+                        const int cnt = __shfl_sync(0xffffffffu, wseed.cnt, k);
+                        const int64_t t0 = __shfl_sync(0xffffffffu, wseed.t0, k);
+                        if (lane < cnt) {
+                            const char* src = reinterpret_cast<const char*>(a.tl + t0 + lane);
+                            char* dst = reinterpret_cast<char*>(&sm.went[k][lane]);
+                            cp_async16(dst, src);
+                            cp_async16(dst + 16, src + 16);
+                        }
+                    }
+                    cp_async_wait_all();
                     __syncwarp();
                     if (wmask == 0) continue;
                 }
                 const int k = __ffs(wmask) - 1;
+                staged = sm.went[k];
                 wmask &= wmask - 1;
                 cur.e = __shfl_sync(0xffffffffu, wseed.e, k);
                 cur.first = __shfl_sync(0xffffffffu, wseed.first, k);
@@ -431,7 +480,7 @@ __global__ void __launch_bounds__(kCleanBlock)
                 cur.t0 = __shfl_sync(0xffffffffu, wseed.t0, k);
             }
             __syncwarp();
-            const int r = pop_edge(a, cur, ws, sw, err, diag);
+            const int r = pop_edge(a, cur, staged, ws, sw, err, diag);
             if (r < 0) break;
             removed += (unsigned long long)r;
         }
@@ -545,8 +594,10 @@ int initial_clean(rtr_graph* g, double eps)
                                             (int64_t)grid_for(1 << 30, kCleanBlock, 8));
         blocks = std::max(blocks, 1);
         ktime_begin(g, KT_CLEAN_UNITS);
-        k_clean_units<<<blocks, kCleanBlock, 0, s>>>(ca, units, order, nu, stacks, next_unit,
-                                                     (unsigned*)(g->ctr + 1), g->ctr, g->ctr + 2);
+        const size_t smem = sizeof(WarpSmem) * kCleanWarps;
+        RTR_CUDA_TRY(cudaFuncSetAttribute(k_clean_units, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_clean_units<<<blocks, kCleanBlock, smem, s>>>(ca, units, order, nu, stacks, next_unit,
+                                                        (unsigned*)(g->ctr + 1), g->ctr, g->ctr + 2);
         ktime_end(g, KT_CLEAN_UNITS);
         g->launches += 1;
         RTR_CUDA_TRY(cudaGetLastError());
