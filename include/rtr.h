@@ -45,8 +45,9 @@ enum rtr_status {
 
 enum rtr_flags {
     RTR_FLAG_SIMPLIFY = 1,     /* drop self-loops and duplicate pairs instead of rejecting them */
-    RTR_FLAG_RTREX_OUTPUTS = 2 /* rtr_run_file also writes what the sequential RTRex CLI writes besides the
-                                  decomposition: connected-components-<name>-* and amazon_cleaned_edges.txt */
+    RTR_FLAG_RTREX_OUTPUTS = 2, /* rtr_run_file also writes what the sequential RTRex CLI writes besides the
+                                   decomposition: connected-components-<name>-* and amazon_cleaned_edges.txt */
+    RTR_FLAG_EXPAND = 4         /* rtr_run_file_ex also runs expandClusters (the RTRex driver's mode e) */
 };
 
 /* Library version string and the calling thread's last error message. */
@@ -185,6 +186,37 @@ int rtr_get_kernel_ms(const rtr_graph* g, double* ms, int n);
 int rtr_count_noalloc(const int64_t* d_offsets, const int32_t* d_nbors, int64_t n, double* d_perEdge,
                       double* d_perVertex, uint32_t* d_support, int64_t* d_total, void* stream);
 
+/* Cluster expansion after rtr_extract: every cluster that has one vertex joins
+ * the cluster holding most of its neighbours (the one whose count first
+ * reaches the maximum in neighbour order) when that count exceeds `threshold`;
+ * its score is that count / its degree.  Votes read the extraction's cluster
+ * map; statistics are recomputed.  *num_scores receives the number of scored
+ * (moved) vertices.  Not defined for a batch handle (RTR_ERR_ARG).
+ * Replaces: expandClusters (RTRex_Sequential/Escape/Decomposition.h:958-1008),
+ *           called by the RTRex driver in mode e (clustering/RTRex.cpp:196-201). */
+int rtr_expand(rtr_graph* g, int64_t threshold, int64_t* num_scores);
+
+/* Copy the expanded clusters: the extraction's clusters, same count and order,
+ * with statistics nv/ne/cut recomputed and members vert[off[k] .. off[k+1]) in
+ * the order the reference's unordered_set iterates them after the moves
+ * (clusters emptied by a move have nv 0).  cluster_of[v] is v's cluster or -1
+ * when v is in none (only possible with threshold <= 0).  Any pointer may be
+ * NULL.  Sizes: nv/ne/cut[n_clusters], off[n_clusters+1], vert[n], cluster_of[n].
+ * Replaces: the vector<Cluster> returned by expandClusters (Decomposition.h:958). */
+int rtr_get_expanded(const rtr_graph* g, int64_t* nv, int64_t* ne, int64_t* cut, int64_t* off, int64_t* vert,
+                     int64_t* cluster_of);
+
+/* The scores of the moved vertices in ascending vertex order: *num_scores
+ * receives their number; vertices[num_scores] and scores[num_scores] are
+ * filled when non-NULL.
+ * Replaces: the std::map<VertexIdx,double> scores of expandClusters (Decomposition.h:958). */
+int rtr_get_scores(const rtr_graph* g, int64_t* num_scores, int64_t* vertices, double* scores);
+
+/* Write <name>-{decomposition,stats,freq,cut}.txt of the expanded clusters as
+ * printDecomposition does and <name>-scores.txt as printScores does
+ * (RTRex_Sequential/clustering/RTRex.cpp:19-118, :120-135, :199-200). */
+int rtr_write_expanded(const rtr_graph* g, const char* name);
+
 /* Write <name>-decomposition.txt, -stats.txt, -freq.txt and -cut.txt exactly as
  * printDecomposition does (RTRex_Sequential/clustering/RTRex.cpp:19-118,
  * RTRex_CUDA/main.cu:57-108), and print its summary lines to stdout. */
@@ -202,6 +234,13 @@ void rtr_free(void* p);
  * Replaces: RTRex_CUDA main (RTRex_CUDA/main.cu:343-391) with prefix "RTRex-CUDA-",
  *           and RTRex main's decomposition output (RTRex.cpp:176-194) with "RTRex-". */
 int rtr_run_file(const char* graph_path, const char* name, double eps, int device, const char* prefix, int flags);
+
+/* rtr_run_file with the RTRex driver's mode e: with RTR_FLAG_EXPAND in flags it
+ * also expands the clusters at `threshold` and writes
+ * <prefix>expanded-<name>-{decomposition,stats,freq,cut,scores}.txt.
+ * Replaces: RTRex <graph> <name> <eps> e <threshold> (RTRex.cpp:141-206). */
+int rtr_run_file_ex(const char* graph_path, const char* name, double eps, int device, const char* prefix,
+                    int flags, int64_t threshold);
 
 #ifdef __cplusplus
 }

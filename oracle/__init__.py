@@ -54,6 +54,9 @@ def lib():
         L.orc_extract.argtypes = [_i64, _i64p, _i64p, _i64p, ctypes.c_double, _f64p, _f64p, _u32p,
                                   ctypes.POINTER(_i64), _u8p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]
         L.orc_extract.restype = _i64
+        L.orc_expand.argtypes = [_i64, _i64p, _i64p, _i64, _i64p, _i64p, _i64p, _i64p, _i64p,
+                                 ctypes.POINTER(_i64), _i64p, _f64p]
+        L.orc_expand.restype = _i64
         L.orc_selfcheck_counts.argtypes = [ctypes.POINTER(_i64)] * 3
         L.orc_selfcheck_reset.argtypes = []
         _lib = L
@@ -178,6 +181,26 @@ def extract(c: Csr, s: State, eps: float):
     cl = Clusters(seed[:k].copy(), nv[:k].copy(), ne[:k].copy(), cut[:k].copy(), off[:k + 1].copy(),
                   vert[:c.n].copy())
     return cl, State(pe[:c.m2], pv[:c.n], sup[:c.m2], int(tot.value), st[:c.m2])
+
+
+def expand(c: Csr, threshold: int):
+    """expandClusters on the clusters of the last :func:`extract` call.
+
+    Returns ``(clusters, score_vertices, score_values)``; the clusters keep the
+    extraction's count and order (emptied singletons have no members) and the
+    ``seed`` field holds -1 (expandClusters does not track seeds)."""
+    n1 = max(1, c.n)
+    nv, ne, cut = (np.zeros(n1, np.int64) for _ in range(3))
+    off = np.zeros(n1 + 1, np.int64)
+    vert = np.zeros(n1, np.int64)
+    sv = np.zeros(n1, np.int64)
+    sx = np.zeros(n1, np.float64)
+    ns = _i64(0)
+    k = lib().orc_expand(c.n, c.offsets, _nb(c), int(threshold), nv, ne, cut, off, vert,
+                         ctypes.byref(ns), sv, sx)
+    cl = Clusters(np.full(k, -1, np.int64), nv[:k].copy(), ne[:k].copy(), cut[:k].copy(),
+                  off[:k + 1].copy(), vert[:off[k]].copy())
+    return cl, sv[:ns.value].copy(), sx[:ns.value].copy()
 
 
 def selfcheck_counts():

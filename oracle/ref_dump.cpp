@@ -7,7 +7,7 @@
 // the restated oracle (rtr_oracle.cpp) and the CUDA path can be pinned against
 // the reference bit for bit.  It is never linked into the product.
 //
-// Usage: rtr_ref_dump <escape-graph-file> <eps> <out-dir>
+// Usage: rtr_ref_dump <escape-graph-file> <eps> <out-dir> [threshold ...]
 //
 // Files written into <out-dir>:
 //   csr_offsets.i64, csr_nbors.i64          makeCSR result  (Graph.cpp:344-384)
@@ -18,6 +18,10 @@
 //   clusters.txt                            disjointExtract  (Decomposition.h:538-940)
 //       one line per cluster in creation order:
 //       "<nVertices> <nEdges> <cut> : <v> <v> ..."  (vertices in set iteration order)
+//   expanded_<t>.txt, scores_<t>.txt        expandClusters   (Decomposition.h:958-1008)
+//       for each threshold argument t, as the RTRex driver calls it in mode e
+//       (RTRex.cpp:196-201): the expanded clusters in the same line format and
+//       the singleton scores as "<v> <score as %a>" in map order
 #include "Escape/GraphIO.h"
 #include "Escape/Graph.h"
 #include "Escape/Decomposition.h"
@@ -84,5 +88,21 @@ int main(int argc, char** argv)
         fprintf(f, "\n");
     }
     fclose(f);
+
+    for (int a = 4; a < argc; ++a) {
+        const int thr = atoi(argv[a]);
+        std::map<VertexIdx, double> scores;
+        std::vector<Cluster> ex = expandClusters(&cg, dec, cmap, thr, scores);
+        FILE* fe = fopen(("expanded_" + std::to_string(thr) + ".txt").c_str(), "w");
+        for (const Cluster& c : ex) {
+            fprintf(fe, "%" PRId64 " %" PRId64 " %" PRId64 " :", c.nVertices, c.nEdges, c.cut);
+            for (VertexIdx v : c.vertices) fprintf(fe, " %" PRId64, v);
+            fprintf(fe, "\n");
+        }
+        fclose(fe);
+        FILE* fs = fopen(("scores_" + std::to_string(thr) + ".txt").c_str(), "w");
+        for (const auto& e : scores) fprintf(fs, "%" PRId64 " %a\n", e.first, e.second);
+        fclose(fs);
+    }
     return 0;
 }

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <map>
 #include <set>
 #include <stack>
 #include <unordered_set>
@@ -47,6 +48,11 @@ struct Pr {
 };
 
 int64_t g_missing = 0, g_badstatus = 0, g_residual = 0;
+
+// The member sets of the last orc_extract call, in creation order, kept as the
+// containers themselves: expandClusters continues inserting into them, and the
+// iteration order after those inserts depends on each set's bucket state.
+std::vector<std::unordered_set<int64_t>> g_last_sets;
 
 // deleteAndClean, Decomposition.h:147-283.  Pops the LIFO stack; every popped
 // edge removes its live triangles (no 'N' edge), subtracting the triangle
@@ -242,6 +248,7 @@ int64_t orc_extract(int64_t n, const int64_t* offsets, const int64_t* nbors, con
     };
     int64_t ncl = 0, nout = 0;
     cl_off[0] = 0;
+    g_last_sets.clear();
     for (int64_t i = 0; i < n; ++i) {
         const int64_t u = order[i].first;
         const int64_t degu = order[i].second;
@@ -331,6 +338,7 @@ int64_t orc_extract(int64_t n, const int64_t* offsets, const int64_t* nbors, con
         for (int64_t z : members) cl_vert[nout++] = z;
         cl_off[ncl + 1] = nout;
         ++ncl;
+        g_last_sets.push_back(members);  // decomposition.push_back(next_clus): a copy
 
         std::stack<Pr> todo;
         for (int64_t z : members)
@@ -343,6 +351,70 @@ int64_t orc_extract(int64_t n, const int64_t* offsets, const int64_t* nbors, con
         delete_and_clean(g, st, pe, pv, sup, total, todo, eps, nullptr, nullptr);
     }
     return ncl;
+}
+
+int64_t orc_expand(int64_t n, const int64_t* offsets, const int64_t* nbors, int64_t threshold,
+                   int64_t* cl_nv, int64_t* cl_ne, int64_t* cl_cut, int64_t* cl_off, int64_t* cl_vert,
+                   int64_t* n_scores, int64_t* sc_vertex, double* sc_value)
+{
+    // expandClusters, Decomposition.h:958-1008.  The decomposition and the
+    // cluster map arrive by value: the sets are copies of the extraction's
+    // (copies keep iteration order and bucket count) and the map is never
+    // updated, so every vote reads the extraction's assignment.
+    std::vector<std::unordered_set<int64_t>> dec = g_last_sets;
+    const int64_t k = (int64_t)dec.size();
+    std::vector<int64_t> cmap(n, -1);
+    std::vector<int64_t> nv0(k);
+    for (int64_t c = 0; c < k; ++c) {
+        nv0[c] = (int64_t)dec[c].size();  // nVertices as populateStats left it
+        for (int64_t z : dec[c]) cmap[z] = c;
+    }
+    std::map<int64_t, double> scores;
+    for (int64_t i = 0; i < k; ++i) {
+        if (nv0[i] > 1) continue;
+        const int64_t v = *dec[i].cbegin();
+        std::map<int64_t, int64_t> counts;
+        int64_t best = -1;
+        int64_t max_score = threshold;
+        const int64_t deg = offsets[v + 1] - offsets[v];
+        for (int64_t j = offsets[v]; j < offsets[v + 1]; ++j) {
+            const int64_t u = nbors[j];
+            if (cmap[u] == -1) continue;
+            const int64_t c = cmap[u];
+            const int64_t cnt = ++counts[c];
+            if (cnt > max_score) {
+                best = c;
+                max_score = cnt;
+            }
+        }
+        if (best == -1) continue;
+        dec[best].insert(v);
+        dec[i].erase(v);
+        scores[v] = (double)max_score / deg;
+    }
+    int64_t nout = 0;
+    cl_off[0] = 0;
+    for (int64_t c = 0; c < k; ++c) {
+        int64_t ne = 0, cut = 0;
+        for (int64_t z : dec[c])
+            for (int64_t j = offsets[z]; j < offsets[z + 1]; ++j) {
+                if (dec[c].count(nbors[j])) ++ne;
+                else ++cut;
+            }
+        cl_nv[c] = (int64_t)dec[c].size();
+        cl_ne[c] = ne / 2;
+        cl_cut[c] = cut;
+        for (int64_t z : dec[c]) cl_vert[nout++] = z;
+        cl_off[c + 1] = nout;
+    }
+    int64_t ns = 0;
+    for (const auto& e : scores) {
+        sc_vertex[ns] = e.first;
+        sc_value[ns] = e.second;
+        ++ns;
+    }
+    *n_scores = ns;
+    return k;
 }
 
 void orc_selfcheck_counts(int64_t* missing_edge, int64_t* bad_status, int64_t* residual)

@@ -11,6 +11,7 @@
  *   orc_count          commonNbr                 RTRex_Sequential/Escape/Decomposition.h:42-117
  *   orc_initial_clean  initialClean (mode s)     Decomposition.h:302-460 (+ deleteAndClean :147-283)
  *   orc_extract        disjointExtract loop      Decomposition.h:566-919 (+ populateStats :473-491)
+ *   orc_expand         expandClusters            Decomposition.h:958-1008
  *
  * Status bytes use the reference's characters: 'Y' alive, 'S' on the
  * deletion stack, 'N' deleted.  support[] is an integer companion the
@@ -53,6 +54,17 @@ int64_t orc_extract(int64_t n, const int64_t* offsets, const int64_t* nbors, con
                     int64_t* total, uint8_t* status,
                     int64_t* cl_seed, int64_t* cl_nv, int64_t* cl_ne, int64_t* cl_cut,
                     int64_t* cl_off, int64_t* cl_vert);
+
+/* expandClusters (Decomposition.h:958-1008) applied to the clusters of the last
+ * orc_extract call (its member sets are kept with their container state).
+ * Writes the same number of clusters, in the same order, with statistics
+ * recomputed and members in set-iteration order (emptied singletons have no
+ * members), and the singleton scores in ascending vertex order
+ * (std::map<VertexIdx,double> iteration).  cl_* sized as for orc_extract,
+ * sc_* sized n.  Returns the number of clusters. */
+int64_t orc_expand(int64_t n, const int64_t* offsets, const int64_t* nbors, int64_t threshold,
+                   int64_t* cl_nv, int64_t* cl_ne, int64_t* cl_cut, int64_t* cl_off, int64_t* cl_vert,
+                   int64_t* n_scores, int64_t* sc_vertex, double* sc_value);
 
 /* Counters of the reference's self-checks that print and continue
  * (Decomposition.h:158-170 and :273-277), accumulated since the last reset. */

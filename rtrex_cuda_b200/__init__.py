@@ -30,6 +30,8 @@ _LIB_PATH = os.path.join(_HERE, "librtr.so")
 _lib = None
 
 RTR_FLAG_SIMPLIFY = 1
+RTR_FLAG_RTREX_OUTPUTS = 2
+RTR_FLAG_EXPAND = 4
 
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -94,6 +96,12 @@ def lib():
     L.rtr_free.restype = None
     L.rtr_run_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p,
                                ctypes.c_int]
+    L.rtr_run_file_ex.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p,
+                                  ctypes.c_int, _i64]
+    L.rtr_expand.argtypes = [_vp, _i64, P(_i64)]
+    L.rtr_get_expanded.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.rtr_get_scores.argtypes = [_vp, P(_i64), _vp, _vp]
+    L.rtr_write_expanded.argtypes = [_vp, ctypes.c_char_p]
     _lib = L
     return L
 
@@ -285,6 +293,37 @@ class Graph:
     def write_decomposition(self, name: str):
         _check(lib().rtr_write_decomposition(self._h, name.encode()))
 
+    def expand(self, threshold: int) -> int:
+        """expandClusters (the RTRex driver's mode e); returns the number of moved vertices."""
+        t = _i64()
+        _check(lib().rtr_expand(self._h, int(threshold), ctypes.byref(t)))
+        return int(t.value)
+
+    def expanded(self):
+        """(clusters, cluster_of) after :meth:`expand`; ``seed`` holds -1 and
+        ``cluster_of`` is -1 for a vertex in no cluster."""
+        n, k = self.n, self.num_clusters()
+        nv, ne, cut = (np.zeros(max(1, k), np.int64) for _ in range(3))
+        off = np.zeros(k + 1, np.int64)
+        vert = np.zeros(max(1, n), np.int64)
+        cof = np.zeros(max(1, n), np.int64)
+        _check(lib().rtr_get_expanded(self._h, _ptr(nv), _ptr(ne), _ptr(cut), _ptr(off), _ptr(vert), _ptr(cof)))
+        cl = Clusters(np.full(k, -1, np.int64), nv[:k], ne[:k], cut[:k], off, vert[:off[k]])
+        return cl, cof[:n]
+
+    def scores(self):
+        """(vertices, scores) of the moved vertices, ascending vertex order."""
+        t = _i64()
+        _check(lib().rtr_get_scores(self._h, ctypes.byref(t), None, None))
+        k = int(t.value)
+        v = np.zeros(max(1, k), np.int64)
+        x = np.zeros(max(1, k), np.float64)
+        _check(lib().rtr_get_scores(self._h, ctypes.byref(t), _ptr(v), _ptr(x)))
+        return v[:k], x[:k]
+
+    def write_expanded(self, name: str):
+        _check(lib().rtr_write_expanded(self._h, name.encode()))
+
 
 def load_escape(path: str):
     """Parse an Escape edge list with the library's loader: (n, src, dst)."""
@@ -301,6 +340,12 @@ def load_escape(path: str):
     return int(n.value), src, dst
 
 
-def run_file(path: str, name: str, eps: float, device: int = 0, prefix: str = "RTRex-CUDA-", simplify=False):
-    _check(lib().rtr_run_file(path.encode(), name.encode(), float(eps), int(device), prefix.encode(),
-                              RTR_FLAG_SIMPLIFY if simplify else 0))
+def run_file(path: str, name: str, eps: float, device: int = 0, prefix: str = "RTRex-CUDA-", simplify=False,
+             rtrex_outputs: bool = False, expand: int | None = None):
+    """The drop-in driver.  rtrex_outputs adds the RTRex CLI's components files
+    and survivor dump; expand=T adds its mode e outputs at threshold T."""
+    flags = (RTR_FLAG_SIMPLIFY if simplify else 0) | (RTR_FLAG_RTREX_OUTPUTS if rtrex_outputs else 0)
+    if expand is not None:
+        flags |= RTR_FLAG_EXPAND
+    _check(lib().rtr_run_file_ex(path.encode(), name.encode(), float(eps), int(device), prefix.encode(), flags,
+                                 int(expand or 0)))

@@ -491,6 +491,64 @@ int rtr_get_cluster_of(const rtr_graph* gc, int64_t* cluster_of)
     return copy_i32_as_i64(g, g->cluster_of, g->n, cluster_of);
 }
 
+int rtr_expand(rtr_graph* g, int64_t threshold, int64_t* num_scores)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    const int rc = expand_clusters(g, threshold);
+    if (rc) return rc;
+    if (num_scores) *num_scores = g->x_nscores;
+    return RTR_OK;
+}
+
+int rtr_get_expanded(const rtr_graph* gc, int64_t* nv, int64_t* ne, int64_t* cut, int64_t* off, int64_t* vert,
+                     int64_t* cluster_of)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || g->stage < 4 || !g->expanded) {
+        set_error("clusters are not expanded yet");
+        return RTR_ERR_STATE;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    const int64_t k = g->ncl;
+    std::vector<int64_t> o(k + 1);
+    RTR_CUDA_TRY(cudaMemcpyAsync(o.data(), g->x_off, sizeof(int64_t) * (k + 1), cudaMemcpyDeviceToHost, s));
+    if (ne) RTR_CUDA_TRY(cudaMemcpyAsync(ne, g->x_ne, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, s));
+    if (cut) RTR_CUDA_TRY(cudaMemcpyAsync(cut, g->x_cut, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    int rc = RTR_OK;
+    if (vert && (rc = copy_i32_as_i64(g, g->x_vert, o[k], vert))) return rc;
+    if (cluster_of && (rc = copy_i32_as_i64(g, g->x_cof, g->n, cluster_of))) return rc;
+    if (off)
+        for (int64_t i = 0; i <= k; ++i) off[i] = o[i];
+    if (nv)
+        for (int64_t i = 0; i < k; ++i) nv[i] = o[i + 1] - o[i];
+    return RTR_OK;
+}
+
+int rtr_get_scores(const rtr_graph* gc, int64_t* num_scores, int64_t* vertices, double* scores)
+{
+    rtr_graph* g = const_cast<rtr_graph*>(gc);
+    if (!g || g->stage < 4 || !g->expanded) {
+        set_error("clusters are not expanded yet");
+        return RTR_ERR_STATE;
+    }
+    if (num_scores) *num_scores = g->x_nscores;
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    int rc = RTR_OK;
+    if (vertices && (rc = copy_i32_as_i64(g, g->x_scv, g->x_nscores, vertices))) return rc;
+    if (scores && g->x_nscores) {
+        RTR_CUDA_TRY(cudaMemcpyAsync(scores, g->x_scx, sizeof(double) * g->x_nscores, cudaMemcpyDeviceToHost,
+                                     g->stream));
+        RTR_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    return RTR_OK;
+}
+
 int rtr_connected_components(rtr_graph* g, int64_t* ncomp)
 {
     if (!g) {

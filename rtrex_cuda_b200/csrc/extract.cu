@@ -555,6 +555,7 @@ int extract_clusters(rtr_graph* g)
     }
     cudaStream_t s = g->stream;
     const int64_t n = g->n, m = g->m, m2 = g->m2;
+    g->expanded = false;
     Scratch sc(g);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

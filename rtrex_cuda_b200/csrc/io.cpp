@@ -226,6 +226,43 @@ int rtr_write_decomposition(const rtr_graph* g, const char* name_c)
     return write_clusters(name_c, n, off, nb, k, nv, ne, coff, vert, cluster_of);
 }
 
+int rtr_write_expanded(const rtr_graph* g, const char* name_c)
+{
+    if (!g || !name_c) {
+        rtr::set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    int64_t n = 0, m = 0, k = 0;
+    int rc = rtr_graph_info(g, &n, &m);
+    if (rc) return rc;
+    if ((rc = rtr_num_clusters(g, &k))) return rc;
+    std::vector<int64_t> off(n + 1), nb(2 * m), cluster_of(n);
+    std::vector<int64_t> nv(k), ne(k), cut(k), coff(k + 1), vert(n);
+    if ((rc = rtr_get_csr(g, off.data(), nb.data()))) return rc;
+    if ((rc = rtr_get_expanded(g, nv.data(), ne.data(), cut.data(), coff.data(), vert.data(), cluster_of.data())))
+        return rc;
+    if ((rc = write_clusters(name_c, n, off, nb, k, nv, ne, coff, vert, cluster_of))) return rc;
+    // printScores (RTRex.cpp:120-135): header line, then the std::map in key order.
+    int64_t ns = 0;
+    if ((rc = rtr_get_scores(g, &ns, nullptr, nullptr))) return rc;
+    std::vector<int64_t> sv(ns);
+    std::vector<double> sx(ns);
+    if ((rc = rtr_get_scores(g, &ns, sv.data(), sx.data()))) return rc;
+    printf("\n--------------------------------------------\n");
+    printf("generating singleton scores\n");
+    const std::string name(name_c);
+    FILE* f = fopen((name + "-scores.txt").c_str(), "w");
+    if (!f) {
+        rtr::set_error("could not write %s-scores.txt", name.c_str());
+        return RTR_ERR_IO;
+    }
+    fprintf(f, "Vertex,Score\n");
+    for (int64_t i = 0; i < ns; ++i) fprintf(f, "%" PRId64 ",%f\n", sv[i], sx[i]);
+    fclose(f);
+    printf("\n--------------------------------------------\n");
+    return RTR_OK;
+}
+
 // The components' member order: the reference inserts a component's vertices
 // into an unordered_set in discovery order (Decomposition.h:1038-1056) and
 // prints them in that set's iteration order, so the writer replays the inserts.
@@ -293,6 +330,12 @@ static int write_cleaned_edges(const rtr_graph* g)
 
 int rtr_run_file(const char* graph_path, const char* name, double eps, int device, const char* prefix, int flags)
 {
+    return rtr_run_file_ex(graph_path, name, eps, device, prefix, flags & ~RTR_FLAG_EXPAND, 0);
+}
+
+int rtr_run_file_ex(const char* graph_path, const char* name, double eps, int device, const char* prefix,
+                    int flags, int64_t threshold)
+{
     if (!graph_path || !name) {
         rtr::set_error("null argument");
         return RTR_ERR_ARG;
@@ -324,6 +367,11 @@ int rtr_run_file(const char* graph_path, const char* name, double eps, int devic
         printf("Time for getting the clusters: %gs \n", ms[3] / 1e3);
         printf("Total clusters extracted: %" PRId64 "\n", ncl);
         rc = rtr_write_decomposition(g, (std::string(prefix ? prefix : "") + name).c_str());
+    }
+    if (!rc && (flags & RTR_FLAG_EXPAND)) {
+        int64_t nsc = 0;
+        rc = rtr_expand(g, threshold, &nsc);
+        if (!rc) rc = rtr_write_expanded(g, (std::string(prefix ? prefix : "") + "expanded-" + name).c_str());
     }
     if (!rc && (flags & RTR_FLAG_RTREX_OUTPUTS)) {
         int64_t ncomp = 0;

@@ -48,6 +48,18 @@ struct rtr_graph {
     int64_t* cl_cut = nullptr;     // [ncl] cut edges
     int32_t* cluster_of = nullptr; // [n]
 
+    // expandClusters results (same clusters, creation order; emptied ones have no members)
+    bool expanded = false;
+    int64_t x_threshold = 0;
+    int64_t* x_off = nullptr;     // [ncl+1] into x_vert
+    int32_t* x_vert = nullptr;    // members in set-iteration order
+    int64_t* x_ne = nullptr;      // [ncl]
+    int64_t* x_cut = nullptr;     // [ncl]
+    int32_t* x_cof = nullptr;     // [n] cluster of each vertex, -1 when in none
+    int64_t x_nscores = 0;
+    int32_t* x_scv = nullptr;     // moved vertices, ascending
+    double* x_scx = nullptr;      // their scores
+
     // connected components of the original graph, creation order, BFS discovery order inside
     int64_t ncc = 0;
     int64_t* cc_off = nullptr;   // [ncc+1]
@@ -62,7 +74,7 @@ struct rtr_graph {
     int stage = 0;  // 1 built, 2 counted, 3 cleaned, 4 extracted
 
     // stage timings from CUDA events (ms)
-    float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0, ms_decompose = 0;
+    float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0, ms_decompose = 0, ms_expand = 0;
     // per-kernel device times of the last run (ms), CUDA events on the graph's stream:
     // [0] k_edge_fold [1] k_tri_fill [2] k_vertex_fold [3] k_clean_units [4] k_extract_components
     static constexpr int kTimers = 8;
@@ -108,5 +120,6 @@ int count_triangles(rtr_graph* g);
 int initial_clean(rtr_graph* g, double eps);
 int extract_clusters(rtr_graph* g);
 int connected_components(rtr_graph* g);
+int expand_clusters(rtr_graph* g, int64_t threshold);
 
 }  // namespace rtr

@@ -248,7 +248,11 @@ constexpr int64_t kUsetMaxSize = 101473717;
 // The set's nodes live in caller-provided arrays: node i holds key[i] and the
 // index of the next node in iteration order (-1 ends the list).  bucket[b] names
 // the node *before* bucket b's first node (kBeforeBegin for the list head) or
-// kEmpty.  Node ids are assigned in insertion order.
+// kEmpty.  Node ids are assigned in insertion order (an erased node's id is not
+// reused).  The table grows when an insert takes the size above the current
+// bucket count (max_load_factor 1: the rehash policy's next-resize mark equals
+// the bucket count) and never shrinks, as in the library: after erases, inserts
+// up to the previous size do not rehash.
 struct UsetOrder {
     static constexpr int32_t kEmpty = -1;
     static constexpr int32_t kBeforeBegin = -2;
@@ -258,6 +262,7 @@ struct UsetOrder {
     int64_t nbuckets;
     int32_t head;
     int32_t size;
+    int32_t used;  // node ids handed out
 
     RTR_HD void init(int32_t* k, int32_t* nx, int32_t* b)
     {
@@ -267,7 +272,30 @@ struct UsetOrder {
         nbuckets = 1;
         head = -1;
         size = 0;
+        used = 0;
         bucket[0] = kEmpty;
+    }
+
+    // The state of a set built by `cnt` inserts of distinct keys (no erase),
+    // given its keys in iteration order in key[0..cnt): nodes in list order,
+    // bucket count from the growth schedule, bucket heads from the list (the
+    // list keeps each bucket's nodes together).
+    RTR_HD void init_from_list(int32_t* k, int32_t* nx, int32_t* b, int32_t cnt)
+    {
+        key = k;
+        next = nx;
+        bucket = b;
+        size = used = cnt;
+        nbuckets = cnt ? uset_buckets_after(cnt) : 1;
+        head = cnt ? 0 : -1;
+        for (int64_t i = 0; i < nbuckets; ++i) bucket[i] = kEmpty;
+        int32_t prev = kBeforeBegin;
+        for (int32_t p = 0; p < cnt; ++p) {
+            next[p] = p + 1 < cnt ? p + 1 : -1;
+            const int64_t bk = bkt(key[p]);
+            if (bucket[bk] == kEmpty) bucket[bk] = prev;
+            prev = p;
+        }
     }
     RTR_HD int32_t after(int32_t p) const { return p == kBeforeBegin ? head : next[p]; }
     RTR_HD void set_after(int32_t p, int32_t v)
@@ -321,8 +349,8 @@ struct UsetOrder {
     {
         if (contains(k)) return false;
         const int64_t nb = uset_buckets_after((int64_t)size + 1);
-        if (nb != nbuckets) rehash(nb);
-        const int32_t id = size;
+        if (nb > nbuckets) rehash(nb);
+        const int32_t id = used++;
         key[id] = k;
         const int64_t b = bkt(k);
         if (bucket[b] != kEmpty) {
@@ -335,6 +363,38 @@ struct UsetOrder {
             bucket[b] = kBeforeBegin;
         }
         ++size;
+        return true;
+    }
+
+    // erase(k): unlink k's node, keeping every bucket's before-node valid
+    // (the hashtable's _M_erase / _M_remove_bucket_begin).  Returns false when
+    // k is absent.
+    RTR_HD bool erase(int32_t k)
+    {
+        if (size == 0) return false;
+        const int64_t b = bkt(k);
+        int32_t prev = bucket[b];
+        if (prev == kEmpty) return false;
+        int32_t p = after(prev);
+        while (p != -1 && key[p] != k) {
+            if (next[p] == -1 || bkt(key[next[p]]) != b) return false;
+            prev = p;
+            p = next[p];
+        }
+        if (p == -1) return false;
+        const int32_t nx = next[p];
+        if (prev == bucket[b]) {  // p begins its bucket
+            const int64_t nb = nx != -1 ? bkt(key[nx]) : 0;
+            if (nx == -1 || nb != b) {  // the bucket becomes empty
+                if (nx != -1) bucket[nb] = bucket[b];
+                bucket[b] = kEmpty;
+            }
+        } else if (nx != -1) {
+            const int64_t nb = bkt(key[nx]);
+            if (nb != b) bucket[nb] = prev;
+        }
+        set_after(prev, nx);
+        --size;
         return true;
     }
 };

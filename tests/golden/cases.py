@@ -50,6 +50,24 @@ CASES = {
     "clean_astro": [0.3, 0.1],
 }
 
+# expandClusters (the RTRex driver's mode e) thresholds checked per (case, eps).
+# Thresholds below 1 let singletons join singleton clusters; they pin the
+# oracle's container handling of that case.
+EXPAND = {
+    ("isolated", 0.3): [1],
+    ("k20", 0.3): [1],
+    ("two_k5_bridge", 0.3): [1, 0],
+    ("small_test", 0.3): [1, 2, 0, -1],
+    ("small_test", 0.1): [1],
+    ("sbm_3000_4002", 0.1): [1, 2, 0],
+    ("sbm_3000_4003", 0.1): [2],
+    ("rmat12", 0.3): [1, 3, 0],
+    ("gnp_cliques", 0.3): [1, 2, 3],
+    ("sbm_20000_4000", 0.1): [1, 2],
+    ("chung_lu", 0.3): [1, 2, 0],
+    ("clean_email", 0.3): [2],
+}
+
 # Cases small enough for the fast CPU suite (the rest run in the GPU suite).
 SMALL = ["isolated", "no_edges_but_one", "triangle_free_star", "k4", "k20", "two_k5_bridge", "tie_threshold",
          "eps_zero", "eps_one", "small_test", "sbm_3000_4002", "sbm_3000_4003", "rmat12"]

@@ -11,13 +11,17 @@ graph and records, per stage, the reference's results:
 * files:   sha256 of RTRex-<name>-{decomposition,stats,freq,cut}.txt, of
            connected-components-<name>-*.txt (cc_*) and of amazon_cleaned_edges.txt
            written by the reference CLI (oracle/_ref/RTRex <graph> <name> <eps> s)
+* expand:  per threshold of cases.EXPAND, expandClusters' clusters (same line
+           format as extract), its scores ("<v> <score %a>" lines) and the five
+           RTRex-expanded-<name>-* files of ``RTRex <graph> <name> <eps> e <t>``
 
 small_test (the reference's RTRex_Sequential/Example/small-test.txt graph)
 additionally stores full arrays in small_test.npz.  Graph inputs are either
 regenerated from seeds (rtrex_cuda_b200.graphgen) or, for the bundled data
 files, read from the reference checkout (those cases skip when it is absent).
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py [--reference /root/reference] [--expand-only]
+(--expand-only recomputes only the expand entries of an existing golden.json)
 """
 from __future__ import annotations
 
@@ -36,7 +40,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from rtrex_cuda_b200 import graphgen  # noqa: E402
-from tests.golden.cases import CASES, BUNDLED, load_case  # noqa: E402
+from tests.golden.cases import CASES, BUNDLED, EXPAND, load_case  # noqa: E402
 
 
 def sha(b: bytes) -> str:
@@ -89,13 +93,62 @@ def run_reference_cli(cli_bin: str, path: str, eps: float):
         return out
 
 
+def run_reference_expand(dump_bin: str, cli_bin: str, path: str, eps: float, thresholds):
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        subprocess.run([dump_bin, path, repr(eps), td] + [str(t) for t in thresholds], check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        for t in thresholds:
+            lines = open(os.path.join(td, f"expanded_{t}.txt")).read().splitlines()
+            sc = open(os.path.join(td, f"scores_{t}.txt"), "rb").read()
+            out[str(t)] = {"clusters": len(lines), "digest": sha(cluster_text_from_lines(lines)),
+                           "scores": sha(sc), "nscores": sc.count(b"\n")}
+    for t in thresholds:
+        with tempfile.TemporaryDirectory() as td:
+            subprocess.run([cli_bin, path, "g", repr(eps), "e", str(t)], check=True, cwd=td,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            out[str(t)]["files"] = {kind: sha(open(os.path.join(td, f"RTRex-expanded-g-{kind}.txt"), "rb").read())
+                                    for kind in ("decomposition", "stats", "freq", "cut", "scores")}
+    return out
+
+
+def case_path(name, td, reference):
+    if name in BUNDLED:
+        path = os.path.join(reference, BUNDLED[name])
+        return path if os.path.exists(path) else None
+    n, u, v = load_case(name)
+    path = os.path.join(td, name + ".txt")
+    graphgen.write_escape(path, n, u, v)
+    return path
+
+
+def add_expand(golden, dump_bin, cli_bin, reference):
+    with tempfile.TemporaryDirectory() as td:
+        for (name, eps), thresholds in EXPAND.items():
+            entry = golden["cases"].get(name, {}).get(repr(eps))
+            path = case_path(name, td, reference)
+            if entry is None or path is None:
+                print("skip expand", name, eps)
+                continue
+            entry["expand"] = run_reference_expand(dump_bin, cli_bin, path, eps, thresholds)
+            print("expand", name, eps, {t: e["nscores"] for t, e in entry["expand"].items()}, flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--expand-only", action="store_true")
     args = ap.parse_args()
     dump_bin = os.path.join(ROOT, "oracle", "_ref", "rtr_ref_dump")
-    if not os.path.exists(dump_bin):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.reference}"], check=True)
+    cli_bin = os.path.join(ROOT, "oracle", "_ref", "RTRex")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.reference}"], check=True)
+    if args.expand_only:
+        with open(os.path.join(HERE, "golden.json")) as f:
+            golden = json.load(f)
+        add_expand(golden, dump_bin, cli_bin, args.reference)
+        with open(os.path.join(HERE, "golden.json"), "w") as f:
+            json.dump(golden, f, indent=1, sort_keys=True)
+        return
     golden = {"eps": {}, "cases": {}}
     with tempfile.TemporaryDirectory() as td:
         for name, eps_list in CASES.items():
@@ -117,6 +170,7 @@ def main():
                     np.savez_compressed(os.path.join(HERE, "small_test.npz"), **arrays)
                 print(name, eps, res["count"]["total"], res["clean"]["total"], res["extract"]["clusters"], flush=True)
             golden["cases"][name] = entry
+    add_expand(golden, dump_bin, cli_bin, args.reference)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)
 

@@ -78,6 +78,36 @@ def digests(s0, s1, clusters) -> dict:
     }
 
 
+def c_hexfloat(x: float) -> str:
+    """printf("%a") of a positive normal double, as glibc writes it."""
+    h = float(x).hex()  # '0x1.8000000000000p-1'
+    mant, exp = h[2:].split("p")
+    head, _, frac = mant.partition(".")
+    frac = frac.rstrip("0")
+    return "0x" + head + ("." + frac if frac else "") + "p" + exp
+
+
+def expand_digests(cl, score_v, score_x) -> dict:
+    """Digests of an expandClusters result in the format of golden.json."""
+    lines = cluster_lines(cl.nv, cl.ne, cl.cut, cl.off, cl.vert)
+    sc = "".join(f"{v} {c_hexfloat(x)}\n" for v, x in zip(score_v.tolist(), score_x.tolist()))
+    return {"clusters": len(lines), "digest": sha(("\n".join(lines) + "\n").encode()),
+            "scores": sha(sc.encode()), "nscores": len(score_v)}
+
+
+def oracle_expand(name: str, eps: float, threshold: int):
+    """The oracle's expandClusters on a fresh extraction of the case."""
+    (_, _, _), c, s0, s1, _, _ = oracle_run(name, eps)
+    oracle.extract(c, s1, eps)  # sets the member sets orc_expand continues from
+    return oracle.expand(c, threshold)
+
+
+def expand_cases(names=None):
+    from tests.golden.cases import EXPAND
+    return [(name, eps, t) for (name, eps), ts in EXPAND.items() for t in ts
+            if names is None or name in names]
+
+
 def expected(name: str, eps: float) -> dict:
     return golden()["cases"][name][repr(float(eps))]
 

@@ -69,6 +69,59 @@ static int check_uset(const std::vector<int32_t>& ins, long* cases)
     return 0;
 }
 
+static int same_order(const std::unordered_set<int64_t>& ref, const rtr::UsetOrder& s, const char* what)
+{
+    int32_t p = s.head;
+    for (int64_t x : ref) {
+        if (p == -1 || s.key[p] != x) {
+            printf("USET %s ORDER MISMATCH size=%zu\n", what, ref.size());
+            return 1;
+        }
+        p = s.next[p];
+    }
+    if (p != -1 || (int64_t)ref.size() != s.size || (int64_t)ref.bucket_count() != s.nbuckets) {
+        printf("USET %s SIZE/BUCKETS MISMATCH %zu/%zu vs %d/%ld\n", what, ref.size(), ref.bucket_count(), s.size,
+               (long)s.nbuckets);
+        return 1;
+    }
+    return 0;
+}
+
+// A set built by inserts, copied (the copy keeps iteration order and bucket
+// count), then driven by a mix of inserts and erases: the state rebuilt from the
+// copy's iteration order (init_from_list) follows the library through every step.
+static int check_uset_mixed(const std::vector<int32_t>& base, const std::vector<std::pair<int, int32_t>>& ops,
+                            long* cases)
+{
+    std::unordered_set<int64_t> built;
+    for (int32_t k : base) built.insert(k);
+    std::unordered_set<int64_t> ref = built;
+    size_t cap = built.size() + ops.size() + 1;
+    std::vector<int32_t> key(cap), nxt(cap), bkt(rtr::uset_buckets_after((int64_t)cap) + 1);
+    int32_t cnt = 0;
+    for (int64_t x : built) key[cnt++] = (int32_t)x;
+    rtr::UsetOrder s;
+    s.init_from_list(key.data(), nxt.data(), bkt.data(), cnt);
+    if (same_order(ref, s, "REBUILT")) return 1;
+    for (const auto& op : ops) {
+        bool a, b;
+        if (op.first) {
+            a = ref.insert(op.second).second;
+            b = s.insert(op.second);
+        } else {
+            a = ref.erase(op.second) == 1;
+            b = s.erase(op.second);
+        }
+        if (a != b) {
+            printf("USET %s RESULT MISMATCH\n", op.first ? "INSERT" : "ERASE");
+            return 1;
+        }
+        if (same_order(ref, s, op.first ? "INSERT" : "ERASE")) return 1;
+    }
+    ++*cases;
+    return 0;
+}
+
 // McIlroy's adversary ("A killer adversary for quicksort", 1999): values are
 // fixed lazily during a sort so that every partition is maximally unbalanced.
 // Sorting the resulting input again drives introsort into its heapsort branch.
@@ -145,6 +198,20 @@ int main()
         std::vector<int32_t> ins(n);
         for (int i = 0; i < n; ++i) ins[i] = (int32_t)(rng() % range);
         if (check_uset(ins, &cases)) return 1;
+    }
+    // Rebuilt sets under inserts and erases (cluster expansion: absorbed
+    // singletons join clusters, emptied singletons lose their vertex).
+    for (int rep = 0; rep < 400; ++rep) {
+        int n = 1 + (int)(rng() % (rep < 300 ? 40 : 3000));
+        int range = 1 + (int)(rng() % (rep % 2 ? 64 : 1000000));
+        std::vector<int32_t> base(n);
+        for (int i = 0; i < n; ++i) base[i] = (int32_t)(rng() % range);
+        std::vector<std::pair<int, int32_t>> ops(1 + rng() % (rep < 300 ? 60 : 5000));
+        for (auto& op : ops) {
+            op.first = (rng() % 3) != 0;
+            op.second = (op.first || base.empty()) ? (int32_t)(rng() % range) : base[rng() % base.size()];
+        }
+        if (check_uset_mixed(base, ops, &cases)) return 1;
     }
     printf("OK %ld\n", cases);
     return 0;

@@ -94,3 +94,12 @@ def test_null_arguments_rejected():
     assert L.rtr_graph_destroy(None) == 0
     h = ctypes.c_void_p()
     assert L.rtr_graph_create_from_edges(None, None, 5, 3, 0, 0, ctypes.byref(h)) == 1
+
+
+def test_expand_entry_points_reject_null_graph():
+    L = rtr.lib()
+    n = ctypes.c_int64()
+    assert L.rtr_expand(None, 1, ctypes.byref(n)) == 1
+    assert L.rtr_get_expanded(None, None, None, None, None, None, None) == 5
+    assert L.rtr_get_scores(None, ctypes.byref(n), None, None) == 5
+    assert L.rtr_write_expanded(None, b"x") == 1

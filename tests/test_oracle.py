@@ -38,6 +38,21 @@ def test_oracle_matches_reference_large(name, eps):
     _check(name, eps)
 
 
+@pytest.mark.parametrize("name,eps,thr", helpers.expand_cases(SMALL + ["gnp_cliques", "clean_email"]))
+def test_oracle_expand_matches_reference(name, eps, thr):
+    """expandClusters (mode e): clusters, statistics, member order and scores."""
+    got = helpers.expand_digests(*helpers.oracle_expand(name, eps, thr))
+    assert got == {k: v for k, v in helpers.expected(name, eps)["expand"][str(thr)].items() if k != "files"}
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("name,eps,thr", [c for c in helpers.expand_cases()
+                                          if c[0] not in SMALL + ["gnp_cliques", "clean_email"]])
+def test_oracle_expand_matches_reference_large(name, eps, thr):
+    got = helpers.expand_digests(*helpers.oracle_expand(name, eps, thr))
+    assert got == {k: v for k, v in helpers.expected(name, eps)["expand"][str(thr)].items() if k != "files"}
+
+
 def test_small_test_full_arrays():
     """Every array of the reference's Example graph, not only digests."""
     ref = np.load(os.path.join(helpers.ROOT, "tests", "golden", "small_test.npz"))
