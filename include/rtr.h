@@ -222,6 +222,23 @@ int rtr_write_expanded(const rtr_graph* g, const char* name);
  * RTRex_CUDA/main.cu:57-108), and print its summary lines to stdout. */
 int rtr_write_decomposition(const rtr_graph* g, const char* name);
 
+/* Create a graph straight from Escape edge-list text: the bytes go to the
+ * device and are parsed there (line rules of rtr_load_escape: '#' comments and
+ * blank lines skipped, first data line "n m", then one pair per line, lines past
+ * the m-th pair ignored), then the CSR is built on the device.  Errors and
+ * messages are rtr_load_escape's (RTR_ERR_IO for malformed or short input).
+ * Replaces: loadGraph(path, g, 1, IOFormat::escape) + makeCSR +
+ *           transferGraphToDevice (GraphIO.cpp:19-88, Graph.cpp:344-384,
+ *           RTRex_CUDA/gpu_graph.cuh:47-60). */
+int rtr_graph_create_from_escape_text(const char* text, int64_t len, int device, int flags, rtr_graph** out);
+
+/* The same from a file.  Files above 16 MiB are read in 32 MiB chunks through
+ * two pinned staging buffers, each chunk's copy overlapping the next chunk's
+ * read; the buffers (64 MiB of pinned host memory) are allocated by the first
+ * such call and held until the process exits, and concurrent file parses take
+ * turns on them. */
+int rtr_graph_create_from_escape_file(const char* path, int device, int flags, rtr_graph** out);
+
 /* Parse an Escape edge-list file (first data line "n m", then m lines "u v";
  * '#' and blank lines skipped) into malloc'ed arrays released with rtr_free.
  * Replaces: loadGraph(path, g, 1, IOFormat::escape) (RTRex_Sequential/GraphIO.cpp:19-88);

@@ -98,6 +98,8 @@ def lib():
                                ctypes.c_int]
     L.rtr_run_file_ex.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p,
                                   ctypes.c_int, _i64]
+    L.rtr_graph_create_from_escape_text.argtypes = [ctypes.c_char_p, _i64, ctypes.c_int, ctypes.c_int, P(_vp)]
+    L.rtr_graph_create_from_escape_file.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, P(_vp)]
     L.rtr_expand.argtypes = [_vp, _i64, P(_i64)]
     L.rtr_get_expanded.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.rtr_get_scores.argtypes = [_vp, P(_i64), _vp, _vp]
@@ -171,6 +173,21 @@ class Graph:
         out = np.zeros(k, np.int64)
         _check(lib().rtr_batch_cluster_counts(self._h, _ptr(out)))
         return out
+
+    @classmethod
+    def from_escape_text(cls, text: bytes, device: int = 0, simplify: bool = False) -> "Graph":
+        """Parse Escape edge-list text on the device and build the CSR there."""
+        h = _vp()
+        _check(lib().rtr_graph_create_from_escape_text(text, len(text), int(device),
+                                                        RTR_FLAG_SIMPLIFY if simplify else 0, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_escape_file(cls, path: str, device: int = 0, simplify: bool = False) -> "Graph":
+        h = _vp()
+        _check(lib().rtr_graph_create_from_escape_file(path.encode(), int(device),
+                                                        RTR_FLAG_SIMPLIFY if simplify else 0, ctypes.byref(h)))
+        return cls(h.value)
 
     @classmethod
     def from_csr(cls, offsets, nbors, device: int = 0) -> "Graph":

@@ -163,6 +163,68 @@ int rtr_graph_create_from_edges(const int64_t* src, const int64_t* dst, int64_t 
     return rc;
 }
 
+// Escape text -> device parse -> device CSR, without host edge arrays.
+static int create_from_escape(const char* h_text, FILE* f, int64_t len, const char* what, int device, int flags,
+                              rtr_graph** out)
+{
+    int rc = make_graph(0, device, out);
+    if (rc) return rc;
+    rtr_graph* g = *out;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, g->stream);
+    {
+        Scratch sc(g);
+        int64_t n = 0, m = 0;
+        int64_t *du = nullptr, *dv = nullptr;
+        rc = parse_escape_device(g, sc, h_text, f, len, what, &n, &m, &du, &dv);
+        if (!rc) {
+            g->n = n;
+            rc = build_csr(g, du, dv, m, (flags & RTR_FLAG_SIMPLIFY) != 0);
+        }
+    }
+    cudaEventRecord(e1, g->stream);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&g->ms_build, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) {
+        rtr_graph_destroy(g);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int rtr_graph_create_from_escape_text(const char* text, int64_t len, int device, int flags, rtr_graph** out)
+{
+    if (!out || (!text && len > 0) || len < 0) {
+        set_error("null or negative arguments");
+        return RTR_ERR_ARG;
+    }
+    return create_from_escape(text ? text : "", nullptr, len, "escape text", device, flags, out);
+}
+
+int rtr_graph_create_from_escape_file(const char* path, int device, int flags, rtr_graph** out)
+{
+    if (!path || !out) {
+        set_error("null argument");
+        return RTR_ERR_ARG;
+    }
+    *out = nullptr;
+    FILE* f = fopen(path, "rb");
+    if (!f) {
+        set_error("could not open file %s", path);
+        return RTR_ERR_IO;
+    }
+    fseek(f, 0, SEEK_END);
+    const long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    const int rc = create_from_escape(nullptr, f, sz > 0 ? (int64_t)sz : 0, path, device, flags, out);
+    fclose(f);
+    return rc;
+}
+
 int rtr_batch_create(const int64_t* src, const int64_t* dst, const int64_t* eoff, const int64_t* nverts, int64_t K,
                      int device, int flags, rtr_graph** out)
 {

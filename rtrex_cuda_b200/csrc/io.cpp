@@ -1,6 +1,7 @@
 // Host side of the drop-in surface: the Escape edge-list parser, the
 // decomposition writer and the whole-file driver.
 #include "../../include/rtr.h"
+#include "escape_text.h"
 
 #include <algorithm>
 #include <cerrno>
@@ -17,29 +18,6 @@ void set_error(const char* fmt, ...);
 }
 
 namespace {
-
-bool blank(const char* p, const char* e)
-{
-    for (; p < e; ++p)
-        if (!(*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n' || *p == '\v' || *p == '\f')) return false;
-    return true;
-}
-
-// strtoll-like: skips leading blanks, optional sign, decimal digits.
-bool parse_i64(const char*& p, const char* e, int64_t* out)
-{
-    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f')) ++p;
-    bool neg = false;
-    if (p < e && (*p == '-' || *p == '+')) {
-        neg = *p == '-';
-        ++p;
-    }
-    if (p >= e || *p < '0' || *p > '9') return false;
-    int64_t v = 0;
-    while (p < e && *p >= '0' && *p <= '9') v = v * 10 + (*p++ - '0');
-    *out = neg ? -v : v;
-    return true;
-}
 
 struct ClusterView {
     int64_t nv, ne, idx;
@@ -86,10 +64,10 @@ int rtr_load_escape(const char* path, int64_t* n_out, int64_t* m_out, int64_t** 
         const char* nl = (const char*)memchr(p, '\n', (size_t)(end - p));
         const char* le = nl ? nl : end;
         ++lineno;
-        if (*p != '#' && !blank(p, le)) {
-            const char* q = p;
-            int64_t a = 0, b = 0;
-            if (!parse_i64(q, le, &a) || !parse_i64(q, le, &b)) {
+        int64_t a = 0, b = 0;
+        const int kind = rtr::esc_line(p, le, &a, &b);
+        if (kind != 0) {
+            if (kind == 2) {
                 free(src);
                 free(dst);
                 rtr::set_error("%s:%lld: expected two integers", path, (long long)lineno);
@@ -340,16 +318,13 @@ int rtr_run_file_ex(const char* graph_path, const char* name, double eps, int de
         rtr::set_error("null argument");
         return RTR_ERR_ARG;
     }
-    int64_t n = 0, m = 0;
-    int64_t *src = nullptr, *dst = nullptr;
-    int rc = rtr_load_escape(graph_path, &n, &m, &src, &dst);
-    if (rc) return rc;
-    printf("Loaded graph\nVertices = %" PRId64 "\nEdges = %" PRId64 "\n", n, m);
+    // the text is parsed on the device and the CSR built there
     rtr_graph* g = nullptr;
-    rc = rtr_graph_create_from_edges(src, dst, m, n, device, flags, &g);
-    free(src);
-    free(dst);
+    int rc = rtr_graph_create_from_escape_file(graph_path, device, flags, &g);
     if (rc) return rc;
+    int64_t n = 0, m = 0;
+    rtr_graph_info(g, &n, &m);
+    printf("Loaded graph\nVertices = %" PRId64 "\nEdges = %" PRId64 "\n", n, m);
     int64_t total = 0, left = 0, ncl = 0;
     if (!(rc = rtr_count(g, &total))) {
         printf("Total triangles = %" PRId64 "\n", total);

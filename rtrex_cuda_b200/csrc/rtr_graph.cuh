@@ -6,6 +6,7 @@
 #include "rtr_common.cuh"
 
 #include <cstddef>
+#include <cstdio>
 #include <cstdint>
 #include <vector>
 
@@ -121,5 +122,9 @@ int initial_clean(rtr_graph* g, double eps);
 int extract_clusters(rtr_graph* g);
 int connected_components(rtr_graph* g);
 int expand_clusters(rtr_graph* g, int64_t threshold);
+// Escape text (host buffer h_text, or the open file f when h_text is null) of
+// len bytes -> device edge arrays in sc.
+int parse_escape_device(rtr_graph* g, Scratch& sc, const char* h_text, FILE* f, int64_t len, const char* what,
+                        int64_t* n_out, int64_t* m_out, int64_t** du_out, int64_t** dv_out);
 
 }  // namespace rtr

@@ -103,3 +103,14 @@ def test_expand_entry_points_reject_null_graph():
     assert L.rtr_get_expanded(None, None, None, None, None, None, None) == 5
     assert L.rtr_get_scores(None, ctypes.byref(n), None, None) == 5
     assert L.rtr_write_expanded(None, b"x") == 1
+
+
+def test_escape_device_entry_points_argument_errors(tmp_path):
+    L = rtr.lib()
+    h = ctypes.c_void_p()
+    assert L.rtr_graph_create_from_escape_text(None, 5, 0, 0, ctypes.byref(h)) == 1
+    assert L.rtr_graph_create_from_escape_text(b"1 0\n", -1, 0, 0, ctypes.byref(h)) == 1
+    assert L.rtr_graph_create_from_escape_file(None, 0, 0, ctypes.byref(h)) == 1
+    missing = str(tmp_path / "missing.txt").encode()
+    assert L.rtr_graph_create_from_escape_file(missing, 0, 0, ctypes.byref(h)) == 7
+    assert b"could not open file" in L.rtr_last_error()
