@@ -91,6 +91,11 @@ int rtr_graph_destroy(rtr_graph* g);
 /* n and the number of undirected edges m (nEdges/2 in the reference). */
 int rtr_graph_info(const rtr_graph* g, int64_t* n, int64_t* m);
 
+/* Device memory of the graph: bytes it holds between calls (CSR, state,
+ * results) and the largest temporary working set any call has needed so far.
+ * No counterpart in the reference; used for admission by memory budget. */
+int rtr_get_memory(const rtr_graph* g, int64_t* resident_bytes, int64_t* peak_scratch_bytes);
+
 /* Weighted triangle counting: perEdge, perVertex, support and the total.
  * Replaces: commonNbr (RTRex_Sequential/Escape/Decomposition.h:42-117) and
  *           gpuCommonNbr (RTRex_CUDA/gpu_triangle_count.cuh:23). */
@@ -216,6 +221,54 @@ int rtr_get_scores(const rtr_graph* g, int64_t* num_scores, int64_t* vertices, d
  * printDecomposition does and <name>-scores.txt as printScores does
  * (RTRex_Sequential/clustering/RTRex.cpp:19-118, :120-135, :199-200). */
 int rtr_write_expanded(const rtr_graph* g, const char* name);
+
+/* ---- Request server (no counterpart in the reference) ----------------------
+ * Graphs are registered once (the server keeps a host copy of the edges) and
+ * decomposition requests are submitted against them.  Worker threads admit
+ * requests continuously: the oldest queued request whose graph is idle and whose
+ * device working set fits the HBM budget starts as soon as a worker is free, on
+ * its graph's own stream, so requests overlap on the device.  Graphs stay
+ * resident in HBM after a request and are evicted least-recently-used when the
+ * budget needs room.  Requests for graphs with at most batch_max_edges edges
+ * that wait together (same eps and flags, up to batch_max_graphs) run as one
+ * batched decomposition.  Every result equals the graph's own rtr_decompose. */
+typedef struct rtr_server rtr_server;
+
+typedef struct rtr_request_info {
+    int status;              /* rtr_status of the request */
+    int batched;             /* graphs decomposed together with it (1 = alone) */
+    int64_t n_clusters;      /* clusters extracted */
+    int64_t triangles;       /* triangles before the clean */
+    int64_t triangles_left;  /* triangles after the clean */
+    double t_submit_ms;      /* server clock: submission, */
+    double t_start_ms;       /* start of its device work, */
+    double t_end_ms;         /* results ready on the host */
+    char error[160];         /* message when status != RTR_OK */
+} rtr_request_info;
+
+int rtr_server_create(int device, int64_t hbm_budget_bytes, int workers, int64_t batch_max_edges,
+                      int batch_max_graphs, rtr_server** out);
+
+/* Register a graph (copied); *graph_id is its handle for rtr_server_submit. */
+int rtr_server_add_graph(rtr_server* s, const int64_t* src, const int64_t* dst, int64_t m, int64_t n, int flags,
+                         int64_t* graph_id);
+
+/* Queue a decomposition at eps; cluster_of (n entries, or NULL) receives the
+ * cluster of every vertex (creation order) and must stay valid until the
+ * request is waited for. */
+int rtr_server_submit(rtr_server* s, int64_t graph_id, double eps, int64_t* cluster_of, int64_t* request_id);
+
+/* Block until the request is done and release it; info may be NULL. */
+int rtr_server_wait(rtr_server* s, int64_t request_id, rtr_request_info* info);
+
+/* stats[0..n): resident graphs, bytes in use (resident + reserved), peak bytes
+ * in use, peak requests in flight, evictions, batched launches, requests served
+ * in batches, queued requests. */
+int rtr_server_stats(rtr_server* s, int64_t* stats, int n);
+
+/* Stop the workers after the requests in flight; queued requests are cancelled
+ * (status RTR_ERR_STATE).  Call it after every rtr_server_wait has returned. */
+int rtr_server_destroy(rtr_server* s);
 
 /* Write <name>-decomposition.txt, -stats.txt, -freq.txt and -cut.txt exactly as
  * printDecomposition does (RTRex_Sequential/clustering/RTRex.cpp:19-118,

@@ -100,6 +100,13 @@ def lib():
                                   ctypes.c_int, _i64]
     L.rtr_graph_create_from_escape_text.argtypes = [ctypes.c_char_p, _i64, ctypes.c_int, ctypes.c_int, P(_vp)]
     L.rtr_graph_create_from_escape_file.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, P(_vp)]
+    L.rtr_get_memory.argtypes = [_vp, P(_i64), P(_i64)]
+    L.rtr_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, _i64, ctypes.c_int, P(_vp)]
+    L.rtr_server_add_graph.argtypes = [_vp, _vp, _vp, _i64, _i64, ctypes.c_int, P(_i64)]
+    L.rtr_server_submit.argtypes = [_vp, _i64, ctypes.c_double, _vp, P(_i64)]
+    L.rtr_server_wait.argtypes = [_vp, _i64, _vp]
+    L.rtr_server_stats.argtypes = [_vp, _vp, ctypes.c_int]
+    L.rtr_server_destroy.argtypes = [_vp]
     L.rtr_expand.argtypes = [_vp, _i64, P(_i64)]
     L.rtr_get_expanded.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.rtr_get_scores.argtypes = [_vp, P(_i64), _vp, _vp]
@@ -340,6 +347,78 @@ class Graph:
 
     def write_expanded(self, name: str):
         _check(lib().rtr_write_expanded(self._h, name.encode()))
+
+
+class RequestInfo(ctypes.Structure):
+    """rtr_request_info."""
+    _fields_ = [("status", ctypes.c_int), ("batched", ctypes.c_int), ("n_clusters", ctypes.c_int64),
+                ("triangles", ctypes.c_int64), ("triangles_left", ctypes.c_int64), ("t_submit_ms", ctypes.c_double),
+                ("t_start_ms", ctypes.c_double), ("t_end_ms", ctypes.c_double), ("error", ctypes.c_char * 160)]
+
+
+class Server:
+    """The request server (rtr_server_*): registered graphs resident in HBM under
+    a budget, requests admitted continuously, small graphs batched."""
+
+    STATS = ("resident_graphs", "bytes_in_use", "peak_bytes", "peak_inflight", "evictions", "batches",
+             "batched_requests", "queued")
+
+    def __init__(self, device: int = 0, hbm_budget: int = 120 << 30, workers: int = 8,
+                 batch_max_edges: int = 20000, batch_max_graphs: int = 64):
+        h = _vp()
+        _check(lib().rtr_server_create(int(device), int(hbm_budget), int(workers), int(batch_max_edges),
+                                       int(batch_max_graphs), ctypes.byref(h)))
+        self._h = h.value
+        self._n = []
+        self._bufs = {}
+
+    def add_graph(self, n: int, src, dst, simplify: bool = False) -> int:
+        src = np.ascontiguousarray(src, dtype=np.int64)
+        dst = np.ascontiguousarray(dst, dtype=np.int64)
+        gid = _i64()
+        _check(lib().rtr_server_add_graph(self._h, _ptr(src), _ptr(dst), src.size, int(n),
+                                          RTR_FLAG_SIMPLIFY if simplify else 0, ctypes.byref(gid)))
+        self._n.append(int(n))
+        return int(gid.value)
+
+    def submit(self, graph_id: int, eps: float, cluster_of: bool = True) -> int:
+        n = self._n[graph_id] if 0 <= graph_id < len(self._n) else 0  # unknown ids: the library reports them
+        buf = np.zeros(max(1, n), np.int64) if cluster_of else None
+        rid = _i64()
+        _check(lib().rtr_server_submit(self._h, int(graph_id), float(eps), _ptr(buf), ctypes.byref(rid)))
+        self._bufs[int(rid.value)] = (buf, n)
+        return int(rid.value)
+
+    def wait(self, request_id: int) -> dict:
+        info = RequestInfo()
+        _check(lib().rtr_server_wait(self._h, int(request_id), ctypes.byref(info)))
+        buf, n = self._bufs.pop(int(request_id))
+        out = {f: getattr(info, f) for f, _ in RequestInfo._fields_ if f != "error"}
+        out["error"] = info.error.decode(errors="replace")
+        out["cluster_of"] = None if buf is None else buf[:n]
+        return out
+
+    def stats(self) -> dict:
+        v = np.zeros(8, np.int64)
+        _check(lib().rtr_server_stats(self._h, _ptr(v), 8))
+        return {k: int(x) for k, x in zip(self.STATS, v)}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rtr_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def load_escape(path: str):

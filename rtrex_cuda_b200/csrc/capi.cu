@@ -348,6 +348,17 @@ int rtr_graph_destroy(rtr_graph* g)
     return RTR_OK;
 }
 
+int rtr_get_memory(const rtr_graph* g, int64_t* resident_bytes, int64_t* peak_scratch_bytes)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    if (resident_bytes) *resident_bytes = g->owned_bytes;
+    if (peak_scratch_bytes) *peak_scratch_bytes = g->scratch_peak;
+    return RTR_OK;
+}
+
 int rtr_graph_info(const rtr_graph* g, int64_t* n, int64_t* m)
 {
     if (!g) {

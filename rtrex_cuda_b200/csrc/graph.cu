@@ -46,6 +46,7 @@ void* dev_alloc(rtr_graph* g, size_t bytes)
     if (bytes == 0) bytes = 16;
     if (cudaMallocAsync(&p, bytes, g->stream) != cudaSuccess) return nullptr;
     g->owned.push_back(p);
+    g->owned_bytes += (int64_t)bytes;
     return p;
 }
 
@@ -53,6 +54,7 @@ void dev_free_all(rtr_graph* g)
 {
     for (void* p : g->owned) cudaFreeAsync(p, g->stream);
     g->owned.clear();
+    g->owned_bytes = 0;
 }
 
 void* Scratch::get(size_t bytes)
@@ -61,12 +63,16 @@ void* Scratch::get(size_t bytes)
     if (bytes == 0) bytes = 16;
     if (cudaMallocAsync(&p, bytes, g->stream) != cudaSuccess) return nullptr;
     ptrs.push_back(p);
+    this->bytes += (int64_t)bytes;
+    g->scratch_bytes += (int64_t)bytes;
+    if (g->scratch_bytes > g->scratch_peak) g->scratch_peak = g->scratch_bytes;
     return p;
 }
 
 Scratch::~Scratch()
 {
     for (void* p : ptrs) cudaFreeAsync(p, g->stream);
+    g->scratch_bytes -= bytes;
 }
 
 namespace {

@@ -231,12 +231,13 @@ uint64_t* radix_sort_u64(uint64_t* d_keys, uint64_t* d_alt, int64_t n, int nbits
 
 int grid_for(int64_t work, int block, int blocks_per_sm)
 {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
+    static const int sms = [] {  // initialised once, thread-safe
+        int dev = 0, count = 0;
         cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-    }
+        if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || count <= 0)
+            count = 148;
+        return count;
+    }();
     const int64_t need = (work + block - 1) / block;
     const int64_t cap = (int64_t)sms * blocks_per_sm;
     int64_t g = std::min<int64_t>(need, cap);

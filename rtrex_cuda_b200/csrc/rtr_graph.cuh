@@ -89,6 +89,10 @@ struct rtr_graph {
     long long diag_bad_status = 0;
 
     std::vector<void*> owned;  // device allocations released by rtr_graph_destroy
+    // device bytes: held by the graph (owned), and temporary scratch now / at most
+    int64_t owned_bytes = 0;
+    int64_t scratch_bytes = 0;
+    int64_t scratch_peak = 0;
 };
 
 namespace rtr {
@@ -110,6 +114,7 @@ void dev_free_all(rtr_graph* g);
 struct Scratch {
     rtr_graph* g;
     std::vector<void*> ptrs;
+    int64_t bytes = 0;
     explicit Scratch(rtr_graph* gr) : g(gr) {}
     void* get(size_t bytes);
     ~Scratch();

@@ -114,3 +114,23 @@ def test_escape_device_entry_points_argument_errors(tmp_path):
     missing = str(tmp_path / "missing.txt").encode()
     assert L.rtr_graph_create_from_escape_file(missing, 0, 0, ctypes.byref(h)) == 7
     assert b"could not open file" in L.rtr_last_error()
+
+
+def test_server_entry_points_without_gpu():
+    L = rtr.lib()
+    h = ctypes.c_void_p()
+    assert L.rtr_server_create(0, 1 << 30, 0, 0, 1, ctypes.byref(h)) == 1  # no workers
+    assert L.rtr_server_create(0, 0, 2, 0, 1, ctypes.byref(h)) == 1        # no budget
+    assert L.rtr_server_destroy(None) == 0
+    assert L.rtr_server_wait(None, 1, None) == 1
+    if not torch_cuda_available():
+        assert L.rtr_server_create(0, 1 << 30, 2, 0, 1, ctypes.byref(h)) == 2
+        assert b"no CUDA device" in L.rtr_last_error()
+
+
+def torch_cuda_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
