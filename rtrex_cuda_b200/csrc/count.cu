@@ -17,7 +17,8 @@
 //                  of the two rows -> perEdge fold, live support, triangles with z>v
 //   k_tri_fill     same intersection, writes the edge's triangle list
 //                  {z, fwd(a,z), fwd(b,z), deg z} (used by the clean and for perVertex)
-//   k_vertex_fold  one thread per vertex: perVertex fold from the triangle lists
+//   k_vertex_fold_light / _heavy  perVertex fold from the triangle lists: a thread
+//                  per vertex of degree < 32, a warp per vertex of degree >= 32
 #include "primitives.cuh"
 #include "rtr_graph.cuh"
 
@@ -138,30 +139,100 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
+// Entries of edge c = fwd(x,y) with z > y: [first, tl_off[c+1]).
+__device__ __forceinline__ int64_t first_above(const TriEntry* __restrict__ tl, int64_t lo, int64_t hi, int32_t y)
+{
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (tl[mid].z <= y) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+constexpr int kHeavyDeg = 32;  // vertices of at least this degree are folded by a whole warp
+
+// perVertex[x] = left fold over y in N(x) ascending, then z > y ascending, of the
+// triangle weights (Decomposition.h:95-101).
+//
+// k_vertex_fold_light: one thread per vertex of degree < kHeavyDeg (at most
+// kHeavyDeg^2/2 entries each).
 __global__ void __launch_bounds__(kBlock)
-    k_vertex_fold(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ deg,
-                  const int32_t* __restrict__ partner, int64_t n, const int64_t* __restrict__ tl_off,
-                  const TriEntry* __restrict__ tl, double* __restrict__ pv)
+    k_vertex_fold_light(const int64_t* __restrict__ off, const int32_t* __restrict__ nb,
+                        const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, int64_t n,
+                        const int64_t* __restrict__ tl_off, const TriEntry* __restrict__ tl, double* __restrict__ pv)
 {
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        if (deg[x] >= kHeavyDeg) continue;
         double acc = 0.0;
         for (int64_t i = off[x]; i < off[x + 1]; ++i) {
             const int32_t y = nb[i];
             const int64_t c = (x < y) ? i : (int64_t)partner[i];
-            int64_t lo = tl_off[c];
             const int64_t hi = tl_off[c + 1];
-            if (lo == hi) continue;
-            // first entry with z > y
-            int64_t a = lo, b = hi;
-            while (a < b) {
-                const int64_t mid = (a + b) >> 1;
-                if (tl[mid].z <= y) a = mid + 1;
-                else b = mid;
-            }
-            // the entry's weight is the same integer product's reciprocal
-            for (int64_t p = a; p < hi; ++p) acc += tl[p].wgt;
+            for (int64_t p = first_above(tl, tl_off[c], hi, y); p < hi; ++p) acc += tl[p].wgt;
         }
         pv[x] = acc;
+    }
+}
+
+// k_vertex_fold_heavy: one warp per vertex of degree >= kHeavyDeg, dealt by id
+// modulo the warp count (power-law generators put hubs at neighbouring ids).
+// Per 32 neighbours the lanes find their entry ranges at once; the ranges'
+// entries are then loaded 32 at a time in fold order (each lane finds its range
+// by a 5-step search over the range ends in shared memory), staged in shared
+// memory, and added in order -- only the floating-point chain is sequential.
+constexpr int kHeavyBlock = 128;
+__global__ void __launch_bounds__(kHeavyBlock)
+    k_vertex_fold_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb,
+                        const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, int64_t n,
+                        const int64_t* __restrict__ tl_off, const TriEntry* __restrict__ tl, double* __restrict__ pv)
+{
+    __shared__ int64_t s_end[kHeavyBlock / 32][32];
+    __shared__ int64_t s_beg[kHeavyBlock / 32][32];
+    __shared__ double s_w[kHeavyBlock / 32][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t nwarps = (int64_t)gridDim.x * (kHeavyBlock / 32);
+    for (int64_t hx = (int64_t)blockIdx.x * (kHeavyBlock / 32) + wib; hx < n; hx += nwarps) {
+        if (deg[hx] < kHeavyDeg) continue;  // uniform across the warp
+        const int64_t h0 = off[hx], h1 = off[hx + 1];
+        double acc = 0.0;
+        for (int64_t cb = h0; cb < h1; cb += 32) {
+            const int64_t i = cb + lane;
+            int64_t a = 0, len = 0;
+            if (i < h1) {
+                const int32_t y = nb[i];
+                const int64_t c = (hx < y) ? i : (int64_t)partner[i];
+                const int64_t hi = tl_off[c + 1];
+                a = first_above(tl, tl_off[c], hi, y);
+                len = hi - a;
+            }
+            int64_t end = len;  // inclusive prefix of the range lengths
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t t = __shfl_up_sync(0xffffffffu, end, o);
+                if (lane >= o) end += t;
+            }
+            s_end[wib][lane] = end;
+            s_beg[wib][lane] = a - (end - len);  // entry index = s_beg[owner] + k
+            __syncwarp();
+            const int64_t total = s_end[wib][31];
+            for (int64_t k0 = 0; k0 < total; k0 += 32) {
+                const int64_t k = k0 + lane;
+                if (k < total) {
+                    int lo = 0, hi = 31;  // first lane whose range ends after k
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (s_end[wib][mid] <= k) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    s_w[wib][lane] = tl[s_beg[wib][lo] + k].wgt;
+                }
+                __syncwarp();
+                const int cnt = total - k0 < 32 ? (int)(total - k0) : 32;
+                for (int j = 0; j < cnt; ++j) acc += s_w[wib][j];
+                __syncwarp();
+            }
+        }
+        if (lane == 0) pv[hx] = acc;
     }
 }
 
@@ -225,10 +296,12 @@ int count_triangles(rtr_graph* g)
                                      g->tl_off, g->tl);
     ktime_end(g, KT_TRI_FILL);
     ktime_begin(g, KT_VERTEX_FOLD);
-    k_vertex_fold<<<grid_for(n, kBlock), kBlock, 0, s>>>(g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl,
-                                                          g->pv);
+    k_vertex_fold_light<<<grid_for(n, kBlock), kBlock, 0, s>>>(g->offsets, g->nbors, g->deg, g->partner, n,
+                                                                g->tl_off, g->tl, g->pv);
+    k_vertex_fold_heavy<<<grid_for(1ll << 40, kHeavyBlock, 16), kHeavyBlock, 0, s>>>(
+        g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl, g->pv);
     ktime_end(g, KT_VERTEX_FOLD);
-    g->launches += 2;
+    g->launches += 3;
     RTR_CUDA_TRY(cudaGetLastError());
     cudaEventRecord(e1, s);
     RTR_CUDA_TRY(cudaEventSynchronize(e1));

@@ -181,6 +181,27 @@ def sbm(m_target: int, seed: int, mean_intra=12.0, mean_inter=2.0,
     return n, u, v
 
 
+def served_pool(count: int, seed0: int = 5000, m_lo: float = 1e3, m_hi: float = 1e7):
+    """Graphs for the served form: edge targets log-uniform in [m_lo, m_hi],
+    alternating the G(n,p)+planted-cliques shape (mean degree ~16.7 as at
+    n=10,000, p=0.0016; one 20-clique per 500 vertices) and R-MAT (a,b,c =
+    .57,.19,.19; scale and edge factor chosen for the target), seeds seed0+i.
+    Edge counts land near the targets (R-MAT loses duplicates)."""
+    out = []
+    for i in range(count):
+        rng = np.random.Generator(np.random.PCG64(seed0 + i))
+        m = float(np.exp(rng.uniform(np.log(m_lo), np.log(m_hi))))
+        if i % 2 == 0:
+            n = max(64, int(round(m / 8.35)))
+            out.append(gnp_cliques(n=n, p=16.7 / (n - 1), n_cliques=max(1, n // 500),
+                                   clique_size=min(20, n // 4), seed=seed0 + i))
+        else:
+            scale = max(6, int(round(np.log2(m / 10.0))))
+            ef = max(1, int(round(1.25 * m / (1 << scale))))
+            out.append(rmat(scale=scale, edge_factor=ef, seed=seed0 + i))
+    return out
+
+
 def small_test():
     """A 10-vertex, 19-edge graph with one dense 4-vertex core."""
     pairs = [(1, 7), (3, 6), (1, 2), (0, 1), (1, 3), (1, 6), (1, 4), (3, 4), (2, 0), (2, 9),
