@@ -22,7 +22,10 @@
 //    out for two dependent round trips: (1) the popped edge's 32-byte record
 //    and its triangle-list entries (which carry the triangle weight), then
 //    (2) the records of the two other edges of every triangle and the third
-//    vertex's weight.  The lanes take 32 triangles at a time, update the
+//    vertex's weight.  Lists longer than 32 entries are taken 64 at a time
+//    with the next window's entries fetched during the current window's
+//    records (pop_edge); shorter ones take the single-window path (pop_short).
+//    The lanes take 32 triangles at a time, update the
 //    distinct per-triangle cells in parallel, fold the shared cells (the
 //    popped edge, its two endpoints) in triangle order, and append pushes in
 //    the reference's push order (triangle order, (lower,w) before (higher,w)).
@@ -273,132 +276,223 @@ struct WarpStack {
     int scount;
 };
 
-// Pop one edge: deleteAndClean's loop body (Decomposition.h:152-281) for the
-// whole warp.  Returns the number of triangles removed, or -1 on overflow.
+// 32 consecutive triangle-list entries of a pop (lane k holds entry base+k)
+// with the records of their two other edges and their third vertex's weight.
+struct Group {
+    TriEntry t;
+    EdgeRec r1, r2;  // (lower, z) and (higher, z)
+    double pz;
+    bool valid;
+};
+
+__device__ __forceinline__ void load_group(const CleanArgs& a, Group& g, bool lower_is_a)
+{
+    g.r1.ss = SS_N;
+    g.r2.ss = SS_N;
+    g.pz = 0.0;
+    if (g.valid) {
+        g.r1 = a.rec[lower_is_a ? g.t.raz : g.t.rbz];
+        g.r2 = a.rec[lower_is_a ? g.t.rbz : g.t.raz];
+        g.pz = a.pv[g.t.z];
+    }
+}
+
+struct PopCtx {
+    bool lower_is_a;
+    int32_t lower, higher, dlow, dhigh;
+    double acc_e, acc_u, acc_v;
+    int removed;
+};
+
+// Remove the group's live triangles in list order: per-triangle cells in
+// parallel, the popped edge and its endpoints folded in order, pushes appended
+// in the reference's order.  False on stack overflow.
+__device__ __forceinline__ bool apply_group(const CleanArgs& a, const Group& g, PopCtx& p, WarpStack& ws, double* sw,
+                                            unsigned* err)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int32_t rlw = p.lower_is_a ? g.t.raz : g.t.rbz;
+    const int32_t rhw = p.lower_is_a ? g.t.rbz : g.t.raz;
+    const uint32_t c1 = g.r1.ss & SS_CODE, c2 = g.r2.ss & SS_CODE;
+    const bool live = g.valid && c1 != SS_N && c2 != SS_N;
+    const double wgt = live ? g.t.wgt : 0.0;
+    bool p1 = false, p2 = false;
+    if (live) {
+        const double x1 = g.r1.pe - wgt;
+        const double x2 = g.r2.pe - wgt;
+        p1 = c1 != SS_S && x1 < g.r1.thr;
+        p2 = c2 != SS_S && x2 < g.r2.thr;
+        a.rec[rlw].pe = x1;
+        a.rec[rhw].pe = x2;
+        a.rec[rlw].ss = ((g.r1.ss & SS_SUP) - 1u) | (p1 ? SS_S : c1);
+        a.rec[rhw].ss = ((g.r2.ss & SS_SUP) - 1u) | (p2 ? SS_S : c2);
+        a.pv[g.t.z] = g.pz - wgt;
+    }
+    sw[lane] = wgt;
+    const unsigned lm = __ballot_sync(0xffffffffu, live);
+    const unsigned b1 = __ballot_sync(0xffffffffu, p1);
+    const unsigned b2 = __ballot_sync(0xffffffffu, p2);
+    __syncwarp();
+    // the popped edge and its endpoints accumulate in triangle order
+    for (unsigned mm = lm; mm; mm &= mm - 1) {
+        const double w = sw[__ffs(mm) - 1];
+        p.acc_e -= w;
+        p.acc_u -= w;
+        p.acc_v -= w;
+    }
+    const int np = __popc(b1) + __popc(b2);
+    if (np) {
+        if (ws.scount + np > kSmemStack) {  // spill the shared part, oldest first
+            if (ws.gtop + ws.scount > ws.cap) {
+                if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                return false;
+            }
+            for (int k = lane; k < ws.scount; k += 32) ws.gm[ws.gtop + k] = ws.sm[k];
+            ws.gtop += ws.scount;
+            ws.scount = 0;
+            __syncwarp();
+        }
+        const int before = ws.scount + __popc(b1 & lt) + __popc(b2 & lt);
+        if (p1) ws.sm[before] = StackEntry{rlw, p.lower, g.t.z, p.dlow, g.t.dz, (int32_t)g.r1.cnt, g.r1.t0};
+        if (p2)
+            ws.sm[before + (p1 ? 1 : 0)] = StackEntry{rhw, p.higher, g.t.z, p.dhigh, g.t.dz, (int32_t)g.r2.cnt, g.r2.t0};
+        ws.scount += np;
+    }
+    __syncwarp();
+    p.removed += __popc(lm);
+    return true;
+}
+
+__device__ __forceinline__ void pop_begin(const StackEntry& c, PopCtx& p)
+{
+    const int32_t u = c.first, v = c.second;
+    const bool lo_is_u = c.dfirst < c.dsecond;
+    p.lower = lo_is_u ? u : v;
+    p.higher = lo_is_u ? v : u;
+    p.dlow = lo_is_u ? c.dfirst : c.dsecond;
+    p.dhigh = lo_is_u ? c.dsecond : c.dfirst;
+    p.lower_is_a = p.lower == (u < v ? u : v);  // a = smaller endpoint of the forward edge
+    p.removed = 0;
+}
+
+// The popped edge's own state: lane 0 its support word, lanes 1-3 its weight
+// and its endpoints' weights (issued in the first round trip).
+__device__ __forceinline__ void pop_own_loads(const CleanArgs& a, const StackEntry& c, uint32_t& s_e, double& scal)
+{
+    const int lane = threadIdx.x & 31;
+    s_e = 0;
+    scal = 0.0;
+    if (lane == 0) s_e = a.rec[c.e].ss;
+    else if (lane == 1) scal = a.rec[c.e].pe;
+    else if (lane == 2) scal = a.pv[c.first];
+    else if (lane == 3) scal = a.pv[c.second];
+}
+
+// False when the edge has no live triangle left (it is retired here).
+__device__ __forceinline__ bool pop_own_state(const CleanArgs& a, const StackEntry& c, uint32_t& s_e, double scal,
+                                              PopCtx& p, unsigned long long* diag)
+{
+    const int lane = threadIdx.x & 31;
+    s_e = __shfl_sync(0xffffffffu, s_e, 0) & SS_SUP;
+    p.acc_e = __shfl_sync(0xffffffffu, scal, 1);
+    p.acc_u = __shfl_sync(0xffffffffu, scal, 2);
+    p.acc_v = __shfl_sync(0xffffffffu, scal, 3);
+    if (s_e == 0) {
+        if (lane == 0) {
+            if (fabs(p.acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
+            a.rec[c.e].ss = SS_N;
+        }
+        __syncwarp();
+        return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void pop_end(const CleanArgs& a, const StackEntry& c, uint32_t s_e, const PopCtx& p,
+                                        unsigned long long* diag)
+{
+    if ((threadIdx.x & 31) == 0) {
+        a.rec[c.e].pe = p.acc_e;
+        a.rec[c.e].ss = (s_e - (uint32_t)p.removed) | SS_N;
+        a.pv[c.first] = p.acc_u;
+        a.pv[c.second] = p.acc_v;
+        if (fabs(p.acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
+    }
+    __syncwarp();
+}
+
+// Pop of an edge with at most 32 triangle-list entries: deleteAndClean's loop
+// body (Decomposition.h:152-281) for the whole warp in two dependent round
+// trips -- (1) the edge's record, its endpoints' weights and its entries (a
+// window seed has them staged in shared memory, so its group's records come in
+// this round trip too), then (2) the records of the two other edges of every
+// triangle and the third vertex's weight.  Returns the number of triangles
+// removed, or -1 on overflow.
+__device__ __forceinline__ int pop_short(const CleanArgs& a, const StackEntry& c, const TriEntry* staged,
+                                         WarpStack& ws, double* sw, unsigned* err, unsigned long long* diag)
+{
+    const int lane = threadIdx.x & 31;
+    PopCtx p;
+    pop_begin(c, p);
+    uint32_t s_e;
+    double scal;
+    pop_own_loads(a, c, s_e, scal);
+    Group g;
+    g.valid = lane < c.cnt;
+    g.t = TriEntry{};
+    if (g.valid) g.t = staged ? staged[lane] : a.tl[c.t0 + lane];
+    if (staged) load_group(a, g, p.lower_is_a);
+    if (!pop_own_state(a, c, s_e, scal, p, diag)) return 0;
+    if (!staged) load_group(a, g, p.lower_is_a);
+    if (!apply_group(a, g, p, ws, sw, err)) return -1;
+    pop_end(a, c, s_e, p, diag);
+    return p.removed;
+}
+
+// Pop of an edge with a longer list.  Within a pop the liveness of every
+// triangle is fixed (only the pop itself turns an edge 'N') and the
+// per-triangle cells are distinct, so the list is taken 64 entries per window
+// (two groups of 32): the window's records are loaded together, and the next
+// window's entries (static data) are fetched while they are in flight.
 __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c, const TriEntry* staged, WarpStack& ws,
                                         double* sw, unsigned* err, unsigned long long* diag)
 {
     const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const int32_t e = c.e, u = c.first, v = c.second;
-    const int32_t du = c.dfirst, dv = c.dsecond;
-    // round trip 1: the edge's record, its endpoints' weights, its first 32
-    // triangles -- which a window seed already has in shared memory, so for a
-    // seed the second round trip below is issued together with this one.
-    uint32_t s_e = 0;
-    double scal = 0.0;
-    if (lane == 0) s_e = a.rec[e].ss;
-    else if (lane == 1) scal = a.rec[e].pe;
-    else if (lane == 2) scal = a.pv[u];
-    else if (lane == 3) scal = a.pv[v];
-    TriEntry t{};
-    if (lane < c.cnt) t = staged ? staged[lane] : a.tl[c.t0 + lane];
-    const bool lo_is_u0 = du < dv;
-    const int32_t lower0 = lo_is_u0 ? u : v;
-    const bool lower_is_a0 = lower0 == (u < v ? u : v);
-    EdgeRec q1{}, q2{};
-    double qz = 0.0;
-    if (staged && lane < c.cnt) {
-        q1 = a.rec[lower_is_a0 ? t.raz : t.rbz];
-        q2 = a.rec[lower_is_a0 ? t.rbz : t.raz];
-        qz = a.pv[t.z];
+    PopCtx p;
+    pop_begin(c, p);
+    uint32_t s_e;
+    double scal;
+    pop_own_loads(a, c, s_e, scal);
+    Group g0, g1;
+    g0.valid = lane < c.cnt;
+    g1.valid = 32 + lane < c.cnt;
+    g0.t = TriEntry{};
+    g1.t = TriEntry{};
+    if (g0.valid) g0.t = staged ? staged[lane] : a.tl[c.t0 + lane];
+    if (g1.valid) g1.t = a.tl[c.t0 + 32 + lane];
+    const bool seed_records = staged != nullptr;
+    if (seed_records) load_group(a, g0, p.lower_is_a);
+    if (!pop_own_state(a, c, s_e, scal, p, diag)) return 0;
+    TriEntry n0{}, n1{};
+    for (int base = 0; base < c.cnt; base += 64) {
+        if (base > 0) {
+            g0.t = n0;
+            g1.t = n1;
+            g0.valid = base + lane < c.cnt;
+            g1.valid = base + 32 + lane < c.cnt;
+        }
+        // next window's entries, fetched while this window's records load
+        if (base + 64 + lane < c.cnt) n0 = a.tl[c.t0 + base + 64 + lane];
+        if (base + 96 + lane < c.cnt) n1 = a.tl[c.t0 + base + 96 + lane];
+        if (!(base == 0 && seed_records)) load_group(a, g0, p.lower_is_a);
+        const bool second = base + 32 < c.cnt;
+        if (second) load_group(a, g1, p.lower_is_a);
+        if (!apply_group(a, g0, p, ws, sw, err)) return -1;
+        if (second && !apply_group(a, g1, p, ws, sw, err)) return -1;
     }
-    s_e = __shfl_sync(0xffffffffu, s_e, 0) & SS_SUP;
-    double acc_e = __shfl_sync(0xffffffffu, scal, 1);
-    double acc_u = __shfl_sync(0xffffffffu, scal, 2);
-    double acc_v = __shfl_sync(0xffffffffu, scal, 3);
-    if (s_e == 0) {
-        if (lane == 0) {
-            if (fabs(acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
-            a.rec[e].ss = SS_N;
-        }
-        __syncwarp();
-        return 0;
-    }
-    const bool lo_is_u = du < dv;
-    const int32_t lower = lo_is_u ? u : v;
-    const int32_t higher = lo_is_u ? v : u;
-    const int32_t dlow = lo_is_u ? du : dv;
-    const int32_t dhigh = lo_is_u ? dv : du;
-    const bool lower_is_a = lower == (u < v ? u : v);  // a = smaller endpoint of the forward edge
-    int removed = 0;
-    for (int base = 0; base < c.cnt; base += 32) {
-        const bool valid = base + lane < c.cnt;
-        if (base > 0) t = valid ? a.tl[c.t0 + base + lane] : TriEntry{};
-        const int32_t rlw = lower_is_a ? t.raz : t.rbz;
-        const int32_t rhw = lower_is_a ? t.rbz : t.raz;
-        // round trip 2: both other edges' records and the third vertex's weight
-        EdgeRec r1{}, r2{};
-        r1.ss = SS_N;
-        r2.ss = SS_N;
-        double pz = 0.0;
-        if (valid) {
-            if (base == 0 && staged) {
-                r1 = q1;
-                r2 = q2;
-                pz = qz;
-            } else {
-                r1 = a.rec[rlw];
-                r2 = a.rec[rhw];
-                pz = a.pv[t.z];
-            }
-        }
-        const uint32_t c1 = r1.ss & SS_CODE, c2 = r2.ss & SS_CODE;
-        const bool live = valid && c1 != SS_N && c2 != SS_N;
-        const double wgt = live ? t.wgt : 0.0;
-        bool p1 = false, p2 = false;
-        if (live) {
-            const double x1 = r1.pe - wgt;
-            const double x2 = r2.pe - wgt;
-            p1 = c1 != SS_S && x1 < r1.thr;
-            p2 = c2 != SS_S && x2 < r2.thr;
-            a.rec[rlw].pe = x1;
-            a.rec[rhw].pe = x2;
-            a.rec[rlw].ss = ((r1.ss & SS_SUP) - 1u) | (p1 ? SS_S : c1);
-            a.rec[rhw].ss = ((r2.ss & SS_SUP) - 1u) | (p2 ? SS_S : c2);
-            a.pv[t.z] = pz - wgt;
-        }
-        sw[lane] = wgt;
-        const unsigned lm = __ballot_sync(0xffffffffu, live);
-        const unsigned b1 = __ballot_sync(0xffffffffu, p1);
-        const unsigned b2 = __ballot_sync(0xffffffffu, p2);
-        __syncwarp();
-        // the popped edge and its endpoints accumulate in triangle order
-        for (unsigned mm = lm; mm; mm &= mm - 1) {
-            const double w = sw[__ffs(mm) - 1];
-            acc_e -= w;
-            acc_u -= w;
-            acc_v -= w;
-        }
-        const int np = __popc(b1) + __popc(b2);
-        if (np) {
-            if (ws.scount + np > kSmemStack) {  // spill the shared part, oldest first
-                if (ws.gtop + ws.scount > ws.cap) {
-                    if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_STACK_OVERFLOW);
-                    return -1;
-                }
-                for (int k = lane; k < ws.scount; k += 32) ws.gm[ws.gtop + k] = ws.sm[k];
-                ws.gtop += ws.scount;
-                ws.scount = 0;
-                __syncwarp();
-            }
-            const int before = ws.scount + __popc(b1 & lt) + __popc(b2 & lt);
-            if (p1) ws.sm[before] = StackEntry{rlw, lower, t.z, dlow, t.dz, (int32_t)r1.cnt, r1.t0};
-            if (p2) ws.sm[before + (p1 ? 1 : 0)] = StackEntry{rhw, higher, t.z, dhigh, t.dz, (int32_t)r2.cnt, r2.t0};
-            ws.scount += np;
-        }
-        __syncwarp();
-        removed += __popc(lm);
-    }
-    if (lane == 0) {
-        a.rec[e].pe = acc_e;
-        a.rec[e].ss = (s_e - (uint32_t)removed) | SS_N;
-        a.pv[u] = acc_u;
-        a.pv[v] = acc_v;
-        if (fabs(acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
-    }
-    __syncwarp();
-    return removed;
+    pop_end(a, c, s_e, p, diag);
+    return p.removed;
 }
 
 __global__ void __launch_bounds__(kCleanBlock)
@@ -480,7 +574,8 @@ __global__ void __launch_bounds__(kCleanBlock)
                 cur.t0 = __shfl_sync(0xffffffffu, wseed.t0, k);
             }
             __syncwarp();
-            const int r = pop_edge(a, cur, staged, ws, sw, err, diag);
+            const int r = cur.cnt <= 32 ? pop_short(a, cur, staged, ws, sw, err, diag)
+                                        : pop_edge(a, cur, staged, ws, sw, err, diag);
             if (r < 0) break;
             removed += (unsigned long long)r;
         }
