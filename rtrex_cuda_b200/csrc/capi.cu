@@ -348,6 +348,72 @@ int rtr_graph_destroy(rtr_graph* g)
     return RTR_OK;
 }
 
+int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree)
+{
+    if (!g || gallop_ratio < 1 || heavy_degree < 1) {
+        set_error("rtr_set_tuning: null graph or parameter below 1");
+        return RTR_ERR_ARG;
+    }
+    g->tune_gallop = gallop_ratio;
+    g->tune_heavy = heavy_degree;
+    return RTR_OK;
+}
+
+int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    if (gallop_ratio) *gallop_ratio = g->tune_gallop;
+    if (heavy_degree) *heavy_degree = g->tune_heavy;
+    return RTR_OK;
+}
+
+int rtr_autotune(rtr_graph* g, int* gallop_ratio, int* heavy_degree)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    RTR_CUDA_TRY(cudaSetDevice(g->device));
+    // one counting pass per candidate, timed by the kernels' own events;
+    // coordinate descent: gallop ratio first, then the heavy-vertex degree
+    auto timed = [&](int gal, int heavy, double* ms) -> int {
+        g->tune_gallop = gal;
+        g->tune_heavy = heavy;
+        const int rc = count_triangles(g);
+        if (rc) return rc;
+        *ms = (double)g->kms[KT_EDGE_FOLD] + g->kms[KT_TRI_FILL] + g->kms[KT_VERTEX_FOLD];
+        return RTR_OK;
+    };
+    static const int kGallop[] = {4, 8, 16, 32, 64};
+    static const int kHeavy[] = {8, 16, 32, 64, 128};
+    int best_g = g->tune_gallop, best_h = g->tune_heavy;
+    double best = 1e300, ms = 0;
+    int rc = timed(best_g, best_h, &ms);  // warm-up (first allocation of the lists)
+    if (rc) return rc;
+    for (int gal : kGallop) {
+        if ((rc = timed(gal, best_h, &ms))) return rc;
+        if (ms < best) {
+            best = ms;
+            best_g = gal;
+        }
+    }
+    for (int heavy : kHeavy) {
+        if (heavy == best_h) continue;
+        if ((rc = timed(best_g, heavy, &ms))) return rc;
+        if (ms < best) {
+            best = ms;
+            best_h = heavy;
+        }
+    }
+    if ((rc = timed(best_g, best_h, &ms))) return rc;  // leave the graph counted with the choice
+    if (gallop_ratio) *gallop_ratio = best_g;
+    if (heavy_degree) *heavy_degree = best_h;
+    return RTR_OK;
+}
+
 int rtr_get_memory(const rtr_graph* g, int64_t* resident_bytes, int64_t* peak_scratch_bytes)
 {
     if (!g) {

@@ -25,6 +25,10 @@
 //    vertex's weight.  Lists longer than 32 entries are taken 64 at a time
 //    with the next window's entries fetched during the current window's
 //    records (pop_edge); shorter ones take the single-window path (pop_short).
+//    Entries are read evict-first (each list is read once), so streaming the
+//    lists does not displace the edge records from L2.  (Warming the next
+//    pop's lines with prefetch instructions was measured and costs more on
+//    the single warp's critical path than it saves.)
 //    The lanes take 32 triangles at a time, update the
 //    distinct per-triangle cells in parallel, fold the shared cells (the
 //    popped edge, its two endpoints) in triangle order, and append pushes in
@@ -254,8 +258,20 @@ constexpr int kSmemStack = 256;  // newest stack entries of each warp live in sh
 struct WarpSmem {
     StackEntry stack[kSmemStack];  // cascade stack, newest entries
     TriEntry went[32][32];         // first 32 triangles of each seed in the window
+    StackEntry wseed[32];          // the window's seeds (lane k = k-th seed in pop order)
     double sw[32];                 // per-lane triangle weights of the current chunk
 };
+
+// Streaming read of a triangle-list entry: the clean reads each list once, so
+// entries are loaded evict-first and do not displace the edge records in L2.
+__device__ __forceinline__ TriEntry ld_entry(const TriEntry* p)
+{
+    TriEntry t;
+    int4* d = reinterpret_cast<int4*>(&t);
+    d[0] = __ldcs(reinterpret_cast<const int4*>(p));
+    d[1] = __ldcs(reinterpret_cast<const int4*>(p) + 1);
+    return t;
+}
 
 // Asynchronous 16-byte global -> shared copy (no register round trip); all of
 // a window's copies are issued back to back and waited for once.
@@ -441,7 +457,7 @@ __device__ __forceinline__ int pop_short(const CleanArgs& a, const StackEntry& c
     Group g;
     g.valid = lane < c.cnt;
     g.t = TriEntry{};
-    if (g.valid) g.t = staged ? staged[lane] : a.tl[c.t0 + lane];
+    if (g.valid) g.t = staged ? staged[lane] : ld_entry(a.tl + c.t0 + lane);
     if (staged) load_group(a, g, p.lower_is_a);
     if (!pop_own_state(a, c, s_e, scal, p, diag)) return 0;
     if (!staged) load_group(a, g, p.lower_is_a);
@@ -469,8 +485,8 @@ __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c,
     g1.valid = 32 + lane < c.cnt;
     g0.t = TriEntry{};
     g1.t = TriEntry{};
-    if (g0.valid) g0.t = staged ? staged[lane] : a.tl[c.t0 + lane];
-    if (g1.valid) g1.t = a.tl[c.t0 + 32 + lane];
+    if (g0.valid) g0.t = staged ? staged[lane] : ld_entry(a.tl + c.t0 + lane);
+    if (g1.valid) g1.t = ld_entry(a.tl + c.t0 + 32 + lane);
     const bool seed_records = staged != nullptr;
     if (seed_records) load_group(a, g0, p.lower_is_a);
     if (!pop_own_state(a, c, s_e, scal, p, diag)) return 0;
@@ -483,8 +499,8 @@ __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c,
             g1.valid = base + 32 + lane < c.cnt;
         }
         // next window's entries, fetched while this window's records load
-        if (base + 64 + lane < c.cnt) n0 = a.tl[c.t0 + base + 64 + lane];
-        if (base + 96 + lane < c.cnt) n1 = a.tl[c.t0 + base + 96 + lane];
+        if (base + 64 + lane < c.cnt) n0 = ld_entry(a.tl + c.t0 + base + 64 + lane);
+        if (base + 96 + lane < c.cnt) n1 = ld_entry(a.tl + c.t0 + base + 96 + lane);
         if (!(base == 0 && seed_records)) load_group(a, g0, p.lower_is_a);
         const bool second = base + 32 < c.cnt;
         if (second) load_group(a, g1, p.lower_is_a);
@@ -536,6 +552,7 @@ __global__ void __launch_bounds__(kCleanBlock)
                     bool live_seed = false;
                     if (lane < wn) {
                         wseed = a.seeds[sp - 1 - lane];
+                        sm.wseed[lane] = wseed;
                         const EdgeRec r = a.rec[wseed.e];
                         // Support only decreases: a seed already at 0 is a no-op pop.
                         live_seed = (r.ss & SS_SUP) > 0;
@@ -565,13 +582,7 @@ __global__ void __launch_bounds__(kCleanBlock)
                 const int k = __ffs(wmask) - 1;
                 staged = sm.went[k];
                 wmask &= wmask - 1;
-                cur.e = __shfl_sync(0xffffffffu, wseed.e, k);
-                cur.first = __shfl_sync(0xffffffffu, wseed.first, k);
-                cur.second = __shfl_sync(0xffffffffu, wseed.second, k);
-                cur.dfirst = __shfl_sync(0xffffffffu, wseed.dfirst, k);
-                cur.dsecond = __shfl_sync(0xffffffffu, wseed.dsecond, k);
-                cur.cnt = __shfl_sync(0xffffffffu, wseed.cnt, k);
-                cur.t0 = __shfl_sync(0xffffffffu, wseed.t0, k);
+                cur = sm.wseed[k];
             }
             __syncwarp();
             const int r = cur.cnt <= 32 ? pop_short(a, cur, staged, ws, sw, err, diag)

@@ -18,7 +18,11 @@
 //   k_tri_fill     same intersection, writes the edge's triangle list
 //                  {z, fwd(a,z), fwd(b,z), deg z} (used by the clean and for perVertex)
 //   k_vertex_fold_light / _heavy  perVertex fold from the triangle lists: a thread
-//                  per vertex of degree < 32, a warp per vertex of degree >= 32
+//                  per light vertex, a warp per heavy one
+// Two work-split parameters (g->tune_gallop: the row-length ratio above which an
+// intersection gallops instead of merging; g->tune_heavy: the degree from which
+// a vertex is folded by a warp) change how work is spread, never a result; the
+// autotuner (rtr_autotune) times candidates on the graph itself.
 #include "primitives.cuh"
 #include "rtr_graph.cuh"
 
@@ -32,11 +36,11 @@ constexpr int kBlock = 256;
 // f(z, slot_in_a, slot_in_b).  Skewed pairs gallop the short row into the long.
 template <typename F>
 __device__ __forceinline__ void intersect_rows(const int32_t* __restrict__ nb, int64_t a0, int64_t a1, int64_t b0,
-                                               int64_t b1, F&& f)
+                                               int64_t b1, int gallop, F&& f)
 {
     const int64_t la = a1 - a0, lb = b1 - b0;
     if (la == 0 || lb == 0) return;
-    if (la * 16 < lb || lb * 16 < la) {
+    if (la * gallop < lb || lb * gallop < la) {
         const bool a_short = la <= lb;
         const int64_t s0 = a_short ? a0 : b0, s1 = a_short ? a1 : b1;
         int64_t lo = a_short ? b0 : a0;
@@ -92,7 +96,8 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned lon
 __global__ void __launch_bounds__(kBlock)
     k_edge_fold(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                 const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd, int64_t m, double* __restrict__ pe,
-                uint32_t* __restrict__ sup, int64_t* __restrict__ cnt, unsigned long long* __restrict__ total)
+                uint32_t* __restrict__ sup, int64_t* __restrict__ cnt, unsigned long long* __restrict__ total,
+                int gallop)
 {
     unsigned long long tri = 0;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
@@ -101,7 +106,7 @@ __global__ void __launch_bounds__(kBlock)
         const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
         double acc = 0.0;
         uint32_t c = 0, above = 0;
-        intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], [&](int32_t z, int64_t, int64_t) {
+        intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, [&](int32_t z, int64_t, int64_t) {
             acc += 1.0 / (double)(duv * (int64_t)deg[z]);
             ++c;
             above += (z > v) ? 1u : 0u;
@@ -118,14 +123,14 @@ __global__ void __launch_bounds__(kBlock)
     k_tri_fill(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, const int32_t* __restrict__ fwd,
                const int32_t* __restrict__ frank, int64_t m, const int64_t* __restrict__ tl_off,
-               TriEntry* __restrict__ tl)
+               TriEntry* __restrict__ tl, int gallop)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = fwd[k];
         const int32_t u = esrc[i], v = nb[i];
         const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
         int64_t w = tl_off[i];
-        intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], [&](int32_t z, int64_t pu, int64_t pv) {
+        intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, [&](int32_t z, int64_t pu, int64_t pv) {
             TriEntry t;
             t.z = z;
             t.eaz = (u < z) ? (int32_t)pu : partner[pu];
@@ -150,20 +155,20 @@ __device__ __forceinline__ int64_t first_above(const TriEntry* __restrict__ tl, 
     return lo;
 }
 
-constexpr int kHeavyDeg = 32;  // vertices of at least this degree are folded by a whole warp
 
 // perVertex[x] = left fold over y in N(x) ascending, then z > y ascending, of the
 // triangle weights (Decomposition.h:95-101).
 //
-// k_vertex_fold_light: one thread per vertex of degree < kHeavyDeg (at most
-// kHeavyDeg^2/2 entries each).
+// k_vertex_fold_light: one thread per vertex of degree < heavy (at most
+// heavy^2/2 entries each).
 __global__ void __launch_bounds__(kBlock)
     k_vertex_fold_light(const int64_t* __restrict__ off, const int32_t* __restrict__ nb,
                         const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, int64_t n,
-                        const int64_t* __restrict__ tl_off, const TriEntry* __restrict__ tl, double* __restrict__ pv)
+                        const int64_t* __restrict__ tl_off, const TriEntry* __restrict__ tl, double* __restrict__ pv,
+                        int heavy)
 {
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
-        if (deg[x] >= kHeavyDeg) continue;
+        if (deg[x] >= heavy) continue;
         double acc = 0.0;
         for (int64_t i = off[x]; i < off[x + 1]; ++i) {
             const int32_t y = nb[i];
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
-// k_vertex_fold_heavy: one warp per vertex of degree >= kHeavyDeg, dealt by id
+// k_vertex_fold_heavy: one warp per vertex of degree >= heavy, dealt by id
 // modulo the warp count (power-law generators put hubs at neighbouring ids).
 // Per 32 neighbours the lanes find their entry ranges at once; the ranges'
 // entries are then loaded 32 at a time in fold order (each lane finds its range
@@ -185,7 +190,8 @@ constexpr int kHeavyBlock = 128;
 __global__ void __launch_bounds__(kHeavyBlock)
     k_vertex_fold_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb,
                         const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, int64_t n,
-                        const int64_t* __restrict__ tl_off, const TriEntry* __restrict__ tl, double* __restrict__ pv)
+                        const int64_t* __restrict__ tl_off, const TriEntry* __restrict__ tl, double* __restrict__ pv,
+                        int heavy)
 {
     __shared__ int64_t s_end[kHeavyBlock / 32][32];
     __shared__ int64_t s_beg[kHeavyBlock / 32][32];
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(kHeavyBlock)
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t nwarps = (int64_t)gridDim.x * (kHeavyBlock / 32);
     for (int64_t hx = (int64_t)blockIdx.x * (kHeavyBlock / 32) + wib; hx < n; hx += nwarps) {
-        if (deg[hx] < kHeavyDeg) continue;  // uniform across the warp
+        if (deg[hx] < heavy) continue;  // uniform across the warp
         const int64_t h0 = off[hx], h1 = off[hx + 1];
         double acc = 0.0;
         for (int64_t cb = h0; cb < h1; cb += 32) {
@@ -274,7 +280,8 @@ int count_triangles(rtr_graph* g)
     RTR_CUDA_TRY(cudaMemsetAsync(g->sup, 0, sizeof(uint32_t) * (m2 + 1), s));
     const int ge = grid_for(m, kBlock);
     ktime_begin(g, KT_EDGE_FOLD);
-    k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, m, g->pe, g->sup, cnt, g->ctr);
+    k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, m, g->pe, g->sup, cnt, g->ctr,
+                                      g->tune_gallop);
     ktime_end(g, KT_EDGE_FOLD);
     exclusive_scan_i64(cnt, g->tl_off, m2 + 1, nullptr, tmp, s);
     g->launches += 4;
@@ -293,13 +300,13 @@ int count_triangles(rtr_graph* g)
     g->tl_len = tl_len;
     ktime_begin(g, KT_TRI_FILL);
     k_tri_fill<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd, g->frank, m,
-                                     g->tl_off, g->tl);
+                                     g->tl_off, g->tl, g->tune_gallop);
     ktime_end(g, KT_TRI_FILL);
     ktime_begin(g, KT_VERTEX_FOLD);
     k_vertex_fold_light<<<grid_for(n, kBlock), kBlock, 0, s>>>(g->offsets, g->nbors, g->deg, g->partner, n,
-                                                                g->tl_off, g->tl, g->pv);
+                                                                g->tl_off, g->tl, g->pv, g->tune_heavy);
     k_vertex_fold_heavy<<<grid_for(1ll << 40, kHeavyBlock, 16), kHeavyBlock, 0, s>>>(
-        g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl, g->pv);
+        g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl, g->pv, g->tune_heavy);
     ktime_end(g, KT_VERTEX_FOLD);
     g->launches += 3;
     RTR_CUDA_TRY(cudaGetLastError());

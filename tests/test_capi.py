@@ -134,3 +134,11 @@ def torch_cuda_available():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def test_tuning_entry_points_argument_errors():
+    L = rtr.lib()
+    a, b = ctypes.c_int(), ctypes.c_int()
+    assert L.rtr_set_tuning(None, 16, 32) == 1
+    assert L.rtr_get_tuning(None, ctypes.byref(a), ctypes.byref(b)) == 1
+    assert L.rtr_autotune(None, ctypes.byref(a), ctypes.byref(b)) == 1
