@@ -226,17 +226,29 @@ struct ExtractArgs {
     unsigned long long* diag;
 };
 
-// deleteAndClean for one thread (Decomposition.h:147-283).
-__device__ void delete_and_clean_seq(const ExtractArgs& a, DelEntry* stack, int64_t top, int64_t cap)
+// deleteAndClean (Decomposition.h:147-283) after a cluster is cut out, for the
+// whole warp (all lanes call it with the same arguments): a popped edge's
+// triangle list is taken 32 entries at a time.
+// Within one pop a triangle's liveness is fixed and its two other edges and
+// third vertex are distinct from every other triangle's, so the lanes update
+// those cells in parallel; the popped edge's weight and its endpoints' weights
+// are folded in list order and pushes are appended in list order ((lower, z)
+// before (higher, z)), as the sequential loop does.
+__device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int64_t top, int64_t cap)
 {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     long long removed = 0;
     while (top > 0) {
+        __syncwarp();  // pushes and stores of the previous pop are visible
         const DelEntry d = stack[--top];
         const int32_t e = d.e, u = d.first, v = d.second;
         const uint32_t s_e = a.sup[e];
         if (s_e == 0) {
-            if (fabs(a.pe[e]) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
-            a.st[e] = ST_N;
+            if (lane == 0) {
+                if (fabs(a.pe[e]) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
+                a.st[e] = ST_N;
+            }
             continue;
         }
         const int64_t du = a.deg[u], dv = a.deg[v];
@@ -248,50 +260,75 @@ __device__ void delete_and_clean_seq(const ExtractArgs& a, DelEntry* stack, int6
         const bool lower_is_a = lower == a.esrc[e];
         double acc_e = a.pe[e], acc_u = a.pv[u], acc_v = a.pv[v];
         uint32_t rem = 0;
-        for (int64_t p = a.tl_off[e]; p < a.tl_off[e + 1]; ++p) {
-            const TriEntry t = a.tl[p];
+        const int64_t p1end = a.tl_off[e + 1];
+        bool overflow = false;
+        for (int64_t pb = a.tl_off[e]; pb < p1end; pb += 32) {
+            const int64_t p = pb + lane;
+            const bool valid = p < p1end;
+            TriEntry t{};
+            if (valid) t = a.tl[p];
             const int32_t elw = lower_is_a ? t.eaz : t.ebz;
             const int32_t ehw = lower_is_a ? t.ebz : t.eaz;
-            const uint8_t slw = a.st[elw], shw = a.st[ehw];
-            if (slw == ST_N || shw == ST_N) continue;
-            const double wgt = t.wgt;
-            acc_e -= wgt;
-            const double x1 = a.pe[elw] - wgt;
-            const double x2 = a.pe[ehw] - wgt;
-            a.pe[elw] = x1;
-            a.pe[ehw] = x2;
-            acc_u -= wgt;
-            acc_v -= wgt;
-            a.pv[t.z] -= wgt;
-            a.sup[elw] -= 1u;
-            a.sup[ehw] -= 1u;
-            ++rem;
-            if (slw != ST_S && x1 < a.eps * (1 / (double)(dlow * (int64_t)t.dz))) {
-                if (top >= cap) {
-                    atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
-                    return;
-                }
-                stack[top++] = DelEntry{elw, lower, t.z, 0};
+            uint8_t slw = ST_N, shw = ST_N;
+            if (valid) {
+                slw = a.st[elw];
+                shw = a.st[ehw];
+            }
+            const bool live = valid && slw != ST_N && shw != ST_N;
+            const double wgt = live ? t.wgt : 0.0;
+            bool q1 = false, q2 = false;
+            if (live) {
+                const double x1 = a.pe[elw] - wgt;
+                const double x2 = a.pe[ehw] - wgt;
+                a.pe[elw] = x1;
+                a.pe[ehw] = x2;
+                a.pv[t.z] -= wgt;
+                a.sup[elw] -= 1u;
+                a.sup[ehw] -= 1u;
+                q1 = slw != ST_S && x1 < a.eps * (1 / (double)(dlow * (int64_t)t.dz));
+                q2 = shw != ST_S && x2 < a.eps * (1 / (double)(dhigh * (int64_t)t.dz));
+            }
+            const unsigned lm = __ballot_sync(0xffffffffu, live);
+            const unsigned b1 = __ballot_sync(0xffffffffu, q1);
+            const unsigned b2 = __ballot_sync(0xffffffffu, q2);
+            for (unsigned mm = lm; mm; mm &= mm - 1) {
+                const double w = __shfl_sync(0xffffffffu, wgt, __ffs(mm) - 1);
+                acc_e -= w;
+                acc_u -= w;
+                acc_v -= w;
+            }
+            const int np = __popc(b1) + __popc(b2);
+            if (top + np > cap) {
+                if (lane == 0) atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                overflow = true;
+                break;
+            }
+            const int64_t before = top + __popc(b1 & lt) + __popc(b2 & lt);
+            if (q1) {
+                stack[before] = DelEntry{elw, lower, t.z, 0};
                 a.st[elw] = ST_S;
             }
-            if (shw != ST_S && x2 < a.eps * (1 / (double)(dhigh * (int64_t)t.dz))) {
-                if (top >= cap) {
-                    atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
-                    return;
-                }
-                stack[top++] = DelEntry{ehw, higher, t.z, 0};
+            if (q2) {
+                stack[before + (q1 ? 1 : 0)] = DelEntry{ehw, higher, t.z, 0};
                 a.st[ehw] = ST_S;
             }
+            top += np;
+            rem += (uint32_t)__popc(lm);
+            __syncwarp();
         }
-        a.pe[e] = acc_e;
-        a.pv[u] = acc_u;
-        a.pv[v] = acc_v;
-        a.sup[e] = s_e - rem;
+        if (overflow) return;
+        if (lane == 0) {
+            a.pe[e] = acc_e;
+            a.pv[u] = acc_u;
+            a.pv[v] = acc_v;
+            a.sup[e] = s_e - rem;
+            if (fabs(acc_e) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
+            a.st[e] = ST_N;
+        }
         removed += rem;
-        if (fabs(acc_e) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
-        a.st[e] = ST_N;
     }
-    if (removed) atomicAdd(a.total, (unsigned long long)(-removed));
+    __syncwarp();
+    if (lane == 0 && removed) atomicAdd(a.total, (unsigned long long)(-removed));
 }
 
 // Ascending sort of distinct vertex ids (the std::set iteration order).
@@ -327,27 +364,35 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
                                                             const uint64_t* __restrict__ order, int64_t nc,
                                                             unsigned* __restrict__ next_comp)
 {
-    // One warp per component: lane 0 replays the seed loop.  (Giving each
-    // thread its own component would put the largest components, which are
-    // handed out first, into the same warp and serialise them by divergence.)
+    // One warp per component.  Lane 0 replays the seed loop's sequential parts
+    // (the member set, the candidate ranking, the deletion cascade); the
+    // two-hop scan -- for each pair (v, w) of the seed's neighbours, the rows of
+    // the lower-degree one -- is taken 32 candidates x at a time by the whole
+    // warp: within one pair every x is distinct, so each lane updates its own
+    // triwgt[x] / in2hop[x], and the one shared sum (internal) is folded in
+    // lane order, i.e. in the reference's order, identically on every lane.
+    // (Giving each thread its own component would put the largest components,
+    // which are handed out first, into the same warp and serialise them.)
     const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     while (true) {
         unsigned ci = 0;
         if (lane == 0) ci = atomicAdd(next_comp, 1u);
         ci = __shfl_sync(0xffffffffu, ci, 0);
         if ((int64_t)ci >= nc) return;
-        if (lane != 0) continue;
         const int64_t c = (int64_t)(uint32_t)order[ci];
         const CompDesc cd = comps[c];
         const int64_t vb = cd.vbegin, nv = cd.vcount;
         if (nv == 1) {  // an isolated vertex: a singleton cluster with no edges to delete
-            const int32_t u = a.vlist[vb];
-            a.clustered[u] = 1;
-            a.hdr_seed[vb] = u;
-            a.hdr_start[vb] = vb;
-            a.hdr_size[vb] = 1;
-            a.out_vert[vb] = u;
-            a.ncl[c] = 1;
+            if (lane == 0) {
+                const int32_t u = a.vlist[vb];
+                a.clustered[u] = 1;
+                a.hdr_seed[vb] = u;
+                a.hdr_start[vb] = vb;
+                a.hdr_size[vb] = 1;
+                a.out_vert[vb] = u;
+                a.ncl[c] = 1;
+            }
             continue;
         }
         // The member set hashes vertex ids; in a batch the ids are offset per
@@ -360,26 +405,30 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
         int32_t* twohop = a.twohop + vb;
         Cand* cand = a.cand + vb;
         DelEntry* dstack = a.dstack + cd.sbase;
-        int64_t out = vb;
-        int32_t ncl = 0;
+        int64_t out = vb;   // lane 0
+        int32_t ncl = 0;    // lane 0
+        UsetOrder S;        // lane 0
         for (int64_t idx = 0; idx < nv; ++idx) {
+            __syncwarp();  // lane 0's writes of the previous seed are visible
             const int32_t u = a.vlist[vb + idx];
             if (a.clustered[u]) continue;
             const int64_t du = a.deg[u];
-            UsetOrder S;
-            S.init(ukey, unext, ubucket);
-            S.insert(u - base);
-            a.clustered[u] = 1;
             const int64_t r0 = a.off[u], r1 = a.off[u + 1];
-            for (int64_t j = r0; j < r1; ++j) {
-                if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
-                const int32_t v = a.nb[j];
-                S.insert(v - base);
-                a.nbd[v] = 1;
-                a.clustered[v] = 1;
+            if (lane == 0) {
+                S.init(ukey, unext, ubucket);
+                S.insert(u - base);
+                a.clustered[u] = 1;
+                for (int64_t j = r0; j < r1; ++j) {
+                    if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
+                    const int32_t v = a.nb[j];
+                    S.insert(v - base);
+                    a.nbd[v] = 1;
+                    a.clustered[v] = 1;
+                }
             }
-            double internal = 0;
-            int64_t n2 = 0;
+            __syncwarp();
+            double internal = 0;  // the same value on every lane
+            int64_t n2 = 0;       // likewise
             const double thr = (double)du / a.eps;
             for (int64_t j = r0; j < r1; ++j) {
                 if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
@@ -394,87 +443,110 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
                     internal += 1.0 / (double)(du * dv * dw);
                     const int32_t lower = (dv < dw) ? v : w;
                     const int32_t higher = (dv < dw) ? w : v;
-                    for (int64_t l = a.off[lower]; l < a.off[lower + 1]; ++l) {
-                        if (a.st[fwd_slot(lower, l, a.nb, a.partner)] == ST_N) continue;
-                        const int32_t x = a.nb[l];
-                        if (x == lower || x == higher || x == u) continue;
-                        const int64_t lh = find_slot(a.off, a.nb, higher, x);
-                        if (lh < 0 || a.st[fwd_slot(higher, lh, a.nb, a.partner)] == ST_N) continue;
-                        const double wgt = 1.0 / (double)((int64_t)a.deg[x] * dv * dw);
-                        if (a.nbd[x]) {
-                            if (x > v && x > w) internal += wgt;
-                            continue;
+                    const int64_t l1 = a.off[lower + 1];
+                    for (int64_t lb = a.off[lower]; lb < l1; lb += 32) {
+                        const int64_t l = lb + lane;
+                        bool ok = false, in_nbd = false;
+                        int32_t x = 0;
+                        double wgt = 0.0;
+                        if (l < l1 && a.st[fwd_slot(lower, l, a.nb, a.partner)] != ST_N) {
+                            x = a.nb[l];
+                            if (x != lower && x != higher && x != u) {
+                                const int64_t lh = find_slot(a.off, a.nb, higher, x);
+                                if (lh >= 0 && a.st[fwd_slot(higher, lh, a.nb, a.partner)] != ST_N) {
+                                    ok = true;
+                                    wgt = 1.0 / (double)((int64_t)a.deg[x] * dv * dw);
+                                    in_nbd = a.nbd[x] != 0;
+                                }
+                            }
                         }
-                        if (!a.in2hop[x]) {
-                            a.in2hop[x] = 1;
-                            twohop[n2++] = x;
+                        // candidates inside the neighbourhood feed internal, in order
+                        const unsigned im = __ballot_sync(0xffffffffu, ok && in_nbd && x > v && x > w);
+                        for (unsigned mm = im; mm; mm &= mm - 1) internal += __shfl_sync(0xffffffffu, wgt, __ffs(mm) - 1);
+                        // the others are two-hop candidates: distinct x, one lane each
+                        bool fresh = false;
+                        if (ok && !in_nbd) {
+                            fresh = !a.in2hop[x];
+                            if (fresh) a.in2hop[x] = 1;
+                            a.triwgt[x] += wgt;
                         }
-                        a.triwgt[x] += wgt;
+                        const unsigned fm = __ballot_sync(0xffffffffu, fresh);
+                        if (fresh) twohop[n2 + __popc(fm & lt)] = x;
+                        n2 += __popc(fm);
+                        __syncwarp();  // the next chunk or pair may touch the same x from another lane
                     }
                 }
             }
-            sort_ids(twohop, n2);
-            double potential = 0;
-            for (int64_t k = 0; k < n2; ++k) {
-                const int32_t x = twohop[k];
-                cand[k].vertex = x;
-                cand[k].pad = 0;
-                cand[k].wgt = a.triwgt[x];
-                potential += a.triwgt[x];
-                a.triwgt[x] = 0;
-                a.in2hop[x] = 0;
-            }
-            introsort(cand, cand + n2, [](const Cand& p, const Cand& q) { return p.wgt > q.wgt; });
-            double ratio = internal / (internal + potential);
-            int64_t maxind = -1;
-            double num = 0, den = 0;
-            for (int64_t k = 0; k < n2; ++k) {
-                num += cand[k].wgt;
-                den += a.pv[cand[k].vertex];
-                const double nr = (internal + num) / (internal + potential + den);
-                if (nr > ratio) {
-                    ratio = nr;
-                    maxind = k;
+            int fail = 0;
+            int64_t ntop = 0;  // deletion stack built by lane 0, replayed by the warp
+            if (lane == 0) {
+                sort_ids(twohop, n2);
+                double potential = 0;
+                for (int64_t k = 0; k < n2; ++k) {
+                    const int32_t x = twohop[k];
+                    cand[k].vertex = x;
+                    cand[k].pad = 0;
+                    cand[k].wgt = a.triwgt[x];
+                    potential += a.triwgt[x];
+                    a.triwgt[x] = 0;
+                    a.in2hop[x] = 0;
                 }
-            }
-            for (int64_t k = 0; k <= maxind; ++k) {
-                S.insert(cand[k].vertex - base);
-                a.clustered[cand[k].vertex] = 1;
-            }
-            // The reference clears the bit of every neighbour of u (Decomposition.h:879-883).
-            // Only the alive ones were set, and a dead neighbour may belong to another
-            // component that a different thread is processing right now, so clear
-            // exactly the bits this seed set.
-            for (int64_t j = r0; j < r1; ++j)
-                if (a.st[fwd_slot(u, j, a.nb, a.partner)] != ST_N) a.nbd[a.nb[j]] = 0;
-
-            if (out + S.size > vb + nv || ncl >= nv) {  // clusters must partition the component
-                atomicOr(a.err, (unsigned)DEV_ERR_SCRATCH);
-                break;
-            }
-            a.hdr_seed[vb + ncl] = u;
-            a.hdr_start[vb + ncl] = out;
-            a.hdr_size[vb + ncl] = S.size;
-            for (int32_t p = S.head; p != -1; p = S.next[p]) a.out_vert[out++] = S.key[p] + base;
-            ++ncl;
-
-            int64_t top = 0;
-            for (int32_t p = S.head; p != -1; p = S.next[p]) {
-                const int32_t z = S.key[p] + base;
-                for (int64_t j = a.off[z]; j < a.off[z + 1]; ++j) {
-                    const int64_t f = fwd_slot(z, j, a.nb, a.partner);
-                    if (a.st[f] != ST_Y) continue;
-                    if (top >= cd.scap) {
-                        atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
-                        break;
+                introsort(cand, cand + n2, [](const Cand& p, const Cand& q) { return p.wgt > q.wgt; });
+                double ratio = internal / (internal + potential);
+                int64_t maxind = -1;
+                double num = 0, den = 0;
+                for (int64_t k = 0; k < n2; ++k) {
+                    num += cand[k].wgt;
+                    den += a.pv[cand[k].vertex];
+                    const double nr = (internal + num) / (internal + potential + den);
+                    if (nr > ratio) {
+                        ratio = nr;
+                        maxind = k;
                     }
-                    dstack[top++] = DelEntry{(int32_t)f, z, a.nb[j], 0};
-                    a.st[f] = ST_S;
+                }
+                for (int64_t k = 0; k <= maxind; ++k) {
+                    S.insert(cand[k].vertex - base);
+                    a.clustered[cand[k].vertex] = 1;
+                }
+                // The reference clears the bit of every neighbour of u (Decomposition.h:879-883).
+                // Only the alive ones were set, and a dead neighbour may belong to another
+                // component that a different thread is processing right now, so clear
+                // exactly the bits this seed set.
+                for (int64_t j = r0; j < r1; ++j)
+                    if (a.st[fwd_slot(u, j, a.nb, a.partner)] != ST_N) a.nbd[a.nb[j]] = 0;
+
+                if (out + S.size > vb + nv || ncl >= nv) {  // clusters must partition the component
+                    atomicOr(a.err, (unsigned)DEV_ERR_SCRATCH);
+                    fail = 1;
+                } else {
+                    a.hdr_seed[vb + ncl] = u;
+                    a.hdr_start[vb + ncl] = out;
+                    a.hdr_size[vb + ncl] = S.size;
+                    for (int32_t p = S.head; p != -1; p = S.next[p]) a.out_vert[out++] = S.key[p] + base;
+                    ++ncl;
+
+                    int64_t top = 0;
+                    for (int32_t p = S.head; p != -1; p = S.next[p]) {
+                        const int32_t z = S.key[p] + base;
+                        for (int64_t j = a.off[z]; j < a.off[z + 1]; ++j) {
+                            const int64_t f = fwd_slot(z, j, a.nb, a.partner);
+                            if (a.st[f] != ST_Y) continue;
+                            if (top >= cd.scap) {
+                                atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                                break;
+                            }
+                            dstack[top++] = DelEntry{(int32_t)f, z, a.nb[j], 0};
+                            a.st[f] = ST_S;
+                        }
+                    }
+                    ntop = top;
                 }
             }
-            delete_and_clean_seq(a, dstack, top, cd.scap);
+            __syncwarp();
+            if (__shfl_sync(0xffffffffu, fail, 0)) break;
+            delete_and_clean_warp(a, dstack, __shfl_sync(0xffffffffu, ntop, 0), cd.scap);
         }
-        a.ncl[c] = ncl;
+        if (lane == 0) a.ncl[c] = ncl;
     }
 }
 
