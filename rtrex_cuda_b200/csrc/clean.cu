@@ -345,14 +345,18 @@ __device__ __forceinline__ bool apply_group(const CleanArgs& a, const Group& g, 
         a.rec[rhw].ss = ((g.r2.ss & SS_SUP) - 1u) | (p2 ? SS_S : c2);
         a.pv[g.t.z] = g.pz - wgt;
     }
-    sw[lane] = wgt;
     const unsigned lm = __ballot_sync(0xffffffffu, live);
     const unsigned b1 = __ballot_sync(0xffffffffu, p1);
     const unsigned b2 = __ballot_sync(0xffffffffu, p2);
+    // live weights packed in lane (= triangle) order, so the fold below reads
+    // fixed slots and only its floating-point chain is sequential
+    if (live) sw[__popc(lm & lt)] = wgt;
     __syncwarp();
     // the popped edge and its endpoints accumulate in triangle order
-    for (unsigned mm = lm; mm; mm &= mm - 1) {
-        const double w = sw[__ffs(mm) - 1];
+    const int nl = __popc(lm);
+#pragma unroll 4
+    for (int k = 0; k < nl; ++k) {
+        const double w = sw[k];
         p.acc_e -= w;
         p.acc_u -= w;
         p.acc_v -= w;

@@ -234,7 +234,7 @@ struct ExtractArgs {
 // those cells in parallel; the popped edge's weight and its endpoints' weights
 // are folded in list order and pushes are appended in list order ((lower, z)
 // before (higher, z)), as the sequential loop does.
-__device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int64_t top, int64_t cap)
+__device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int64_t top, int64_t cap, double* sw)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -291,8 +291,13 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
             const unsigned lm = __ballot_sync(0xffffffffu, live);
             const unsigned b1 = __ballot_sync(0xffffffffu, q1);
             const unsigned b2 = __ballot_sync(0xffffffffu, q2);
-            for (unsigned mm = lm; mm; mm &= mm - 1) {
-                const double w = __shfl_sync(0xffffffffu, wgt, __ffs(mm) - 1);
+            // live weights packed in list order; the fold reads fixed slots
+            if (live) sw[__popc(lm & lt)] = wgt;
+            __syncwarp();
+            const int nl = __popc(lm);
+#pragma unroll 4
+            for (int k = 0; k < nl; ++k) {
+                const double w = sw[k];
                 acc_e -= w;
                 acc_u -= w;
                 acc_v -= w;
@@ -360,7 +365,9 @@ __device__ void sort_ids(int32_t* x, int64_t n)
     }
 }
 
-__global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const CompDesc* __restrict__ comps,
+constexpr int kExtractBlock = 128;
+
+__global__ void __launch_bounds__(kExtractBlock) k_extract_components(ExtractArgs a, const CompDesc* __restrict__ comps,
                                                             const uint64_t* __restrict__ order, int64_t nc,
                                                             unsigned* __restrict__ next_comp)
 {
@@ -375,6 +382,8 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
     // which are handed out first, into the same warp and serialise them.)
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
+    __shared__ double s_fold[kExtractBlock / 32][32];
+    double* sw = s_fold[threadIdx.x >> 5];
     while (true) {
         unsigned ci = 0;
         if (lane == 0) ci = atomicAdd(next_comp, 1u);
@@ -461,8 +470,14 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
                             }
                         }
                         // candidates inside the neighbourhood feed internal, in order
-                        const unsigned im = __ballot_sync(0xffffffffu, ok && in_nbd && x > v && x > w);
-                        for (unsigned mm = im; mm; mm &= mm - 1) internal += __shfl_sync(0xffffffffu, wgt, __ffs(mm) - 1);
+                        const bool inner = ok && in_nbd && x > v && x > w;
+                        const unsigned im = __ballot_sync(0xffffffffu, inner);
+                        if (im) {
+                            if (inner) sw[__popc(im & lt)] = wgt;
+                            __syncwarp();
+                            const int ni = __popc(im);
+                            for (int q = 0; q < ni; ++q) internal += sw[q];
+                        }
                         // the others are two-hop candidates: distinct x, one lane each
                         bool fresh = false;
                         if (ok && !in_nbd) {
@@ -544,7 +559,7 @@ __global__ void __launch_bounds__(128) k_extract_components(ExtractArgs a, const
             }
             __syncwarp();
             if (__shfl_sync(0xffffffffu, fail, 0)) break;
-            delete_and_clean_warp(a, dstack, __shfl_sync(0xffffffffu, ntop, 0), cd.scap);
+            delete_and_clean_warp(a, dstack, __shfl_sync(0xffffffffu, ntop, 0), cd.scap, sw);
         }
         if (lane == 0) a.ncl[c] = ncl;
     }
@@ -749,7 +764,7 @@ int extract_clusters(rtr_graph* g)
     RTR_CUDA_TRY(cudaMemsetAsync(a.triwgt, 0, sizeof(double) * (n + 1), s));
     RTR_CUDA_TRY(cudaMemsetAsync(next_comp, 0, sizeof(unsigned) * 2, s));
     {
-        const int blk = 128;
+        const int blk = kExtractBlock;
         const int64_t warps = (nc + 0);  // one component per warp
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((warps + 3) / 4, grid_for(1 << 30, blk, 16)));
         ktime_begin(g, KT_EXTRACT);
