@@ -88,11 +88,14 @@ __global__ void __launch_bounds__(kBlock) k_nl_write(const char* __restrict__ te
 }
 
 // One thread per line: kind (0 skipped, 1 data, 2 malformed data), the two
-// values, the first data line and the first malformed one.
+// values, the first data line and the first malformed one.  The two minima
+// are kept per thread and reduced per warp, so the shared words see one
+// atomic per warp rather than one per line.
 __global__ void k_lines(const char* __restrict__ text, int64_t len, const int64_t* __restrict__ nlpos, int64_t nnl,
                         int64_t L, uint32_t* __restrict__ is_data, int64_t* __restrict__ va, int64_t* __restrict__ vb,
                         unsigned long long* __restrict__ first)
 {
+    unsigned first_data = 0xffffffffu, first_bad = 0xffffffffu;  // line indices are below 2^31
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = i == 0 ? 0 : nlpos[i - 1] + 1;
         const int64_t e = i < nnl ? nlpos[i] : len;
@@ -101,8 +104,14 @@ __global__ void k_lines(const char* __restrict__ text, int64_t len, const int64_
         is_data[i] = kind != 0;
         va[i] = a;
         vb[i] = b;
-        if (kind) atomicMin(&first[0], (unsigned long long)i);
-        if (kind == 2) atomicMin(&first[1], (unsigned long long)i);
+        if (kind && (unsigned)i < first_data) first_data = (unsigned)i;
+        if (kind == 2 && (unsigned)i < first_bad) first_bad = (unsigned)i;
+    }
+    first_data = __reduce_min_sync(0xffffffffu, first_data);
+    first_bad = __reduce_min_sync(0xffffffffu, first_bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (first_data != 0xffffffffu) atomicMin(&first[0], (unsigned long long)first_data);
+        if (first_bad != 0xffffffffu) atomicMin(&first[1], (unsigned long long)first_bad);
     }
 }
 
