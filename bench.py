@@ -441,7 +441,7 @@ def batch_arm(args):
         "config": {"workload": "sbm_batch", "graphs": K, "edges": edges, "eps": args.eps,
                    "desc": "SBM graphs, 4-64 blocks, intra mean degree 12, inter 2, edge targets log-uniform "
                            "in [1K, 200K], seeds 4000+i; disjoint union decomposed in one call",
-                   "autotune": {"gallop_ratio": tuning[0], "heavy_degree": tuning[1]}},
+                   "autotune": {"gallop_ratio": tuning[0], "heavy_degree": tuning[1], "heavy_edge": tuning[2]}},
         "e2e": {"value": K / batched_s, "unit": "graphs/s", "h2d_bytes_per_step": 16 * edges,
                 "d2h_bytes_per_step": 8 * K},
         "plain_per_graph": {"value": K / plain_s, "unit": "graphs/s", "seconds": plain_s},

@@ -98,20 +98,21 @@ int rtr_get_memory(const rtr_graph* g, int64_t* resident_bytes, int64_t* peak_sc
 
 /* Work split of the counting kernels: an intersection gallops the shorter row
  * through the longer when their lengths differ by more than gallop_ratio
- * (otherwise it merges), and a vertex of at least heavy_degree neighbours has
- * its perVertex fold done by a whole warp.  Defaults 16 and 32.  Results are
- * the same bits for every setting; only the time changes.  No counterpart in
- * the reference. */
-int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree);
-int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree);
+ * (otherwise it merges); a vertex of at least heavy_degree neighbours has its
+ * perVertex fold done by a whole warp; an edge whose endpoints' degrees sum to
+ * at least heavy_edge is intersected by a whole warp.  Defaults 16, 32, 1024.
+ * Results are the same bits for every setting; only the time changes.  No
+ * counterpart in the reference. */
+int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree, int heavy_edge);
+int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int* heavy_edge);
 
 /* Autotuner: times the counting pass on this graph for gallop ratios
- * {4,8,16,32,64} and then heavy degrees {8,16,32,64,128} (coordinate descent,
- * each candidate timed by the kernels' CUDA events), keeps the fastest pair in
- * the graph and returns it.  Leaves the graph counted (as after rtr_count).
- * Reuse the pair on similar graphs with rtr_set_tuning.  No counterpart in the
- * reference. */
-int rtr_autotune(rtr_graph* g, int* gallop_ratio, int* heavy_degree);
+ * {4,8,16,32,64}, then heavy degrees {8,16,32,64,128}, then heavy-edge degree
+ * sums {128,256,512,1024,4096,off} (coordinate descent, each candidate timed by
+ * the kernels' CUDA events), keeps the fastest triple in the graph and returns
+ * it.  Leaves the graph counted (as after rtr_count).  Reuse the triple on
+ * similar graphs with rtr_set_tuning.  No counterpart in the reference. */
+int rtr_autotune(rtr_graph* g, int* gallop_ratio, int* heavy_degree, int* heavy_edge);
 
 /* Weighted triangle counting: perEdge, perVertex, support and the total.
  * Replaces: commonNbr (RTRex_Sequential/Escape/Decomposition.h:42-117) and

@@ -101,9 +101,9 @@ def lib():
     L.rtr_graph_create_from_escape_text.argtypes = [ctypes.c_char_p, _i64, ctypes.c_int, ctypes.c_int, P(_vp)]
     L.rtr_graph_create_from_escape_file.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, P(_vp)]
     L.rtr_get_memory.argtypes = [_vp, P(_i64), P(_i64)]
-    L.rtr_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
-    L.rtr_get_tuning.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int)]
-    L.rtr_autotune.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int)]
+    L.rtr_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.rtr_get_tuning.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rtr_autotune.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rtr_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, _i64, ctypes.c_int, P(_vp)]
     L.rtr_server_add_graph.argtypes = [_vp, _vp, _vp, _i64, _i64, ctypes.c_int, P(_i64)]
     L.rtr_server_submit.argtypes = [_vp, _i64, ctypes.c_double, _vp, P(_i64)]
@@ -320,20 +320,20 @@ class Graph:
     def write_decomposition(self, name: str):
         _check(lib().rtr_write_decomposition(self._h, name.encode()))
 
-    def set_tuning(self, gallop_ratio: int, heavy_degree: int):
+    def set_tuning(self, gallop_ratio: int, heavy_degree: int, heavy_edge: int = 1024):
         """Counting work split (results are identical for every setting)."""
-        _check(lib().rtr_set_tuning(self._h, int(gallop_ratio), int(heavy_degree)))
+        _check(lib().rtr_set_tuning(self._h, int(gallop_ratio), int(heavy_degree), int(heavy_edge)))
 
     def tuning(self):
-        a, b = ctypes.c_int(), ctypes.c_int()
-        _check(lib().rtr_get_tuning(self._h, ctypes.byref(a), ctypes.byref(b)))
-        return int(a.value), int(b.value)
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().rtr_get_tuning(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return int(a.value), int(b.value), int(c.value)
 
     def autotune(self):
         """Time the counting pass for candidate work splits; keep and return the fastest."""
-        a, b = ctypes.c_int(), ctypes.c_int()
-        _check(lib().rtr_autotune(self._h, ctypes.byref(a), ctypes.byref(b)))
-        return int(a.value), int(b.value)
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().rtr_autotune(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return int(a.value), int(b.value), int(c.value)
 
     def expand(self, threshold: int) -> int:
         """expandClusters (the RTRex driver's mode e); returns the number of moved vertices."""

@@ -348,18 +348,19 @@ int rtr_graph_destroy(rtr_graph* g)
     return RTR_OK;
 }
 
-int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree)
+int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree, int heavy_edge)
 {
-    if (!g || gallop_ratio < 1 || heavy_degree < 1) {
+    if (!g || gallop_ratio < 1 || heavy_degree < 1 || heavy_edge < 1) {
         set_error("rtr_set_tuning: null graph or parameter below 1");
         return RTR_ERR_ARG;
     }
     g->tune_gallop = gallop_ratio;
     g->tune_heavy = heavy_degree;
+    g->tune_edge = heavy_edge;
     return RTR_OK;
 }
 
-int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree)
+int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int* heavy_edge)
 {
     if (!g) {
         set_error("null graph");
@@ -367,10 +368,11 @@ int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree)
     }
     if (gallop_ratio) *gallop_ratio = g->tune_gallop;
     if (heavy_degree) *heavy_degree = g->tune_heavy;
+    if (heavy_edge) *heavy_edge = g->tune_edge;
     return RTR_OK;
 }
 
-int rtr_autotune(rtr_graph* g, int* gallop_ratio, int* heavy_degree)
+int rtr_autotune(rtr_graph* g, int* gallop_ratio, int* heavy_degree, int* heavy_edge)
 {
     if (!g) {
         set_error("null graph");
@@ -378,10 +380,11 @@ int rtr_autotune(rtr_graph* g, int* gallop_ratio, int* heavy_degree)
     }
     RTR_CUDA_TRY(cudaSetDevice(g->device));
     // one counting pass per candidate, timed by the kernels' own events;
-    // coordinate descent: gallop ratio first, then the heavy-vertex degree
-    auto timed = [&](int gal, int heavy, double* ms) -> int {
+    // coordinate descent over the three parameters in turn
+    auto timed = [&](int gal, int heavy, int edge, double* ms) -> int {
         g->tune_gallop = gal;
         g->tune_heavy = heavy;
+        g->tune_edge = edge;
         const int rc = count_triangles(g);
         if (rc) return rc;
         *ms = (double)g->kms[KT_EDGE_FOLD] + g->kms[KT_TRI_FILL] + g->kms[KT_VERTEX_FOLD];
@@ -389,28 +392,38 @@ int rtr_autotune(rtr_graph* g, int* gallop_ratio, int* heavy_degree)
     };
     static const int kGallop[] = {4, 8, 16, 32, 64};
     static const int kHeavy[] = {8, 16, 32, 64, 128};
-    int best_g = g->tune_gallop, best_h = g->tune_heavy;
+    static const int kEdge[] = {128, 256, 512, 1024, 4096, 1 << 30};
+    int bg = g->tune_gallop, bh = g->tune_heavy, be = g->tune_edge;
     double best = 1e300, ms = 0;
-    int rc = timed(best_g, best_h, &ms);  // warm-up (first allocation of the lists)
+    int rc = timed(bg, bh, be, &ms);  // warm-up (first allocation of the lists)
     if (rc) return rc;
     for (int gal : kGallop) {
-        if ((rc = timed(gal, best_h, &ms))) return rc;
+        if ((rc = timed(gal, bh, be, &ms))) return rc;
         if (ms < best) {
             best = ms;
-            best_g = gal;
+            bg = gal;
         }
     }
     for (int heavy : kHeavy) {
-        if (heavy == best_h) continue;
-        if ((rc = timed(best_g, heavy, &ms))) return rc;
+        if (heavy == bh) continue;
+        if ((rc = timed(bg, heavy, be, &ms))) return rc;
         if (ms < best) {
             best = ms;
-            best_h = heavy;
+            bh = heavy;
         }
     }
-    if ((rc = timed(best_g, best_h, &ms))) return rc;  // leave the graph counted with the choice
-    if (gallop_ratio) *gallop_ratio = best_g;
-    if (heavy_degree) *heavy_degree = best_h;
+    for (int edge : kEdge) {
+        if (edge == be) continue;
+        if ((rc = timed(bg, bh, edge, &ms))) return rc;
+        if (ms < best) {
+            best = ms;
+            be = edge;
+        }
+    }
+    if ((rc = timed(bg, bh, be, &ms))) return rc;  // leave the graph counted with the choice
+    if (gallop_ratio) *gallop_ratio = bg;
+    if (heavy_degree) *heavy_degree = bh;
+    if (heavy_edge) *heavy_edge = be;
     return RTR_OK;
 }
 

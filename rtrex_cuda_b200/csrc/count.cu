@@ -19,9 +19,12 @@
 //                  {z, fwd(a,z), fwd(b,z), deg z} (used by the clean and for perVertex)
 //   k_vertex_fold_light / _heavy  perVertex fold from the triangle lists: a thread
 //                  per light vertex, a warp per heavy one
-// Two work-split parameters (g->tune_gallop: the row-length ratio above which an
-// intersection gallops instead of merging; g->tune_heavy: the degree from which
-// a vertex is folded by a warp) change how work is spread, never a result; the
+//   k_edge_count_heavy / k_tri_fill_heavy / k_pe_fold_heavy  the same for edges
+//                  with deg u + deg v >= g->tune_edge, one warp per edge
+// Three work-split parameters (g->tune_gallop: the row-length ratio above which
+// an intersection gallops instead of merging; g->tune_heavy: the degree from
+// which a vertex is folded by a warp; g->tune_edge: the degree sum from which an
+// edge is intersected by a warp) change how work is spread, never a result; the
 // autotuner (rtr_autotune) times candidates on the graph itself.
 #include "primitives.cuh"
 #include "rtr_graph.cuh"
@@ -79,6 +82,71 @@ __device__ __forceinline__ void intersect_rows(const int32_t* __restrict__ nb, i
     }
 }
 
+__device__ __forceinline__ int64_t lower_bound_row(const int32_t* __restrict__ nb, int64_t lo, int64_t hi, int32_t x)
+{
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (nb[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Lane `lane`'s share of the common neighbours of rows A=[a0,a1) and B=[b0,b1),
+// visited in ascending order: f(z, slot_in_a, slot_in_b).  The shorter row is
+// cut into 32 contiguous pieces and the lane takes piece `lane` together with
+// the part of the longer row between its piece's first value and the next
+// piece's first value, so lane l's common neighbours all precede lane l+1's.
+// Within its part a lane merges, or -- when the rows' lengths differ by more
+// than `gallop` -- binary-searches each of its elements.
+template <typename F>
+__device__ __forceinline__ void warp_intersect_part(const int32_t* __restrict__ nb, int64_t a0, int64_t a1, int64_t b0,
+                                                    int64_t b1, int gallop, int lane, F&& f)
+{
+    const int64_t la = a1 - a0, lb = b1 - b0;
+    if (la == 0 || lb == 0) return;
+    const bool a_short = la <= lb;
+    const int64_t s0 = a_short ? a0 : b0, s1 = a_short ? a1 : b1;
+    const int64_t l0 = a_short ? b0 : a0, l1 = a_short ? b1 : a1;
+    const int64_t ls = s1 - s0, ll = l1 - l0;
+    const int64_t piece = (ls + 31) / 32;
+    const int64_t p0 = s0 + (int64_t)lane * piece;
+    const int64_t p1 = p0 + piece < s1 ? p0 + piece : s1;
+    if (p0 >= p1) return;
+    int64_t lo = lower_bound_row(nb, l0, l1, nb[p0]);
+    const int64_t hi = p1 < s1 ? lower_bound_row(nb, lo, l1, nb[p1]) : l1;
+    if (ls * gallop < ll) {
+        for (int64_t p = p0; p < p1 && lo < hi; ++p) {
+            const int32_t x = nb[p];
+            lo = lower_bound_row(nb, lo, hi, x);
+            if (lo < hi && nb[lo] == x) {
+                if (a_short) f(x, p, lo);
+                else f(x, lo, p);
+                ++lo;
+            }
+        }
+        return;
+    }
+    int64_t i = p0, j = lo;
+    if (j >= hi) return;
+    int32_t x = nb[i], y = nb[j];
+    while (true) {
+        if (x < y) {
+            if (++i >= p1) break;
+            x = nb[i];
+        } else if (x > y) {
+            if (++j >= hi) break;
+            y = nb[j];
+        } else {
+            if (a_short) f(x, i, j);
+            else f(x, j, i);
+            if (++i >= p1 || ++j >= hi) break;
+            x = nb[i];
+            y = nb[j];
+        }
+    }
+}
+
 __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long* dst)
 {
     __shared__ unsigned long long s[kBlock / 32];
@@ -97,12 +165,16 @@ __global__ void __launch_bounds__(kBlock)
     k_edge_fold(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                 const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd, int64_t m, double* __restrict__ pe,
                 uint32_t* __restrict__ sup, int64_t* __restrict__ cnt, unsigned long long* __restrict__ total,
-                int gallop)
+                int gallop, int heavy_edge, int32_t* __restrict__ heavy_list, unsigned* __restrict__ nheavy)
 {
     unsigned long long tri = 0;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = fwd[k];
         const int32_t u = esrc[i], v = nb[i];
+        if (deg[u] + deg[v] >= heavy_edge) {  // a warp takes it (k_edge_count_heavy)
+            heavy_list[atomicAdd(nheavy, 1u)] = (int32_t)k;
+            continue;
+        }
         const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
         double acc = 0.0;
         uint32_t c = 0, above = 0;
@@ -123,11 +195,12 @@ __global__ void __launch_bounds__(kBlock)
     k_tri_fill(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                const int32_t* __restrict__ deg, const int32_t* __restrict__ partner, const int32_t* __restrict__ fwd,
                const int32_t* __restrict__ frank, int64_t m, const int64_t* __restrict__ tl_off,
-               TriEntry* __restrict__ tl, int gallop)
+               TriEntry* __restrict__ tl, int gallop, int heavy_edge)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = fwd[k];
         const int32_t u = esrc[i], v = nb[i];
+        if (deg[u] + deg[v] >= heavy_edge) continue;  // k_tri_fill_heavy
         const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
         int64_t w = tl_off[i];
         intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, [&](int32_t z, int64_t pu, int64_t pv) {
@@ -141,6 +214,105 @@ __global__ void __launch_bounds__(kBlock)
             t.rbz = frank[t.ebz];
             tl[w++] = t;
         });
+    }
+}
+
+// Heavy edges (deg u + deg v >= heavy_edge), one warp each, dealt from the list
+// the light edge fold built.  Counting is integer and order-free, so the lanes
+// split the intersection (warp_intersect_part) and sum; the triangle list is
+// written by the same split, each lane at its prefix offset, which keeps the
+// entries in ascending z; perEdge is then folded from the list in that order
+// (the same left fold over z ascending as the thread path).
+constexpr int kHeavyEdgeBlock = 128;
+
+__global__ void __launch_bounds__(kHeavyEdgeBlock)
+    k_edge_count_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
+                       const int32_t* __restrict__ fwd, const int32_t* __restrict__ heavy_list,
+                       const unsigned* __restrict__ nheavy, int gallop, uint32_t* __restrict__ sup,
+                       int64_t* __restrict__ cnt, unsigned long long* __restrict__ total)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nh = *nheavy;
+    const int64_t nwarps = (int64_t)gridDim.x * (kHeavyEdgeBlock / 32);
+    unsigned long long tri = 0;
+    for (int64_t h = (int64_t)blockIdx.x * (kHeavyEdgeBlock / 32) + (threadIdx.x >> 5); h < nh; h += nwarps) {
+        const int64_t i = fwd[heavy_list[h]];
+        const int32_t u = esrc[i], v = nb[i];
+        unsigned c = 0, above = 0;
+        warp_intersect_part(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, lane, [&](int32_t z, int64_t, int64_t) {
+            ++c;
+            above += (z > v) ? 1u : 0u;
+        });
+        c = __reduce_add_sync(0xffffffffu, c);
+        above = __reduce_add_sync(0xffffffffu, above);
+        if (lane == 0) {
+            sup[i] = c;
+            cnt[i] = c;
+            tri += above;
+        }
+    }
+    if (lane == 0 && tri) atomicAdd(total, tri);
+}
+
+__global__ void __launch_bounds__(kHeavyEdgeBlock)
+    k_tri_fill_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
+                     const int32_t* __restrict__ deg, const int32_t* __restrict__ partner,
+                     const int32_t* __restrict__ fwd, const int32_t* __restrict__ frank,
+                     const int32_t* __restrict__ heavy_list, const unsigned* __restrict__ nheavy, int gallop,
+                     const int64_t* __restrict__ tl_off, TriEntry* __restrict__ tl)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nh = *nheavy;
+    const int64_t nwarps = (int64_t)gridDim.x * (kHeavyEdgeBlock / 32);
+    for (int64_t h = (int64_t)blockIdx.x * (kHeavyEdgeBlock / 32) + (threadIdx.x >> 5); h < nh; h += nwarps) {
+        const int64_t i = fwd[heavy_list[h]];
+        const int32_t u = esrc[i], v = nb[i];
+        const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
+        unsigned c = 0;
+        warp_intersect_part(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, lane,
+                            [&](int32_t, int64_t, int64_t) { ++c; });
+        unsigned incl = c;  // inclusive prefix over lanes
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        int64_t w = tl_off[i] + (int64_t)(incl - c);
+        warp_intersect_part(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, lane,
+                            [&](int32_t z, int64_t pu, int64_t pv) {
+                                TriEntry t;
+                                t.z = z;
+                                t.eaz = (u < z) ? (int32_t)pu : partner[pu];
+                                t.ebz = (v < z) ? (int32_t)pv : partner[pv];
+                                t.dz = deg[z];
+                                t.wgt = 1.0 / (double)(duv * (int64_t)t.dz);
+                                t.raz = frank[t.eaz];
+                                t.rbz = frank[t.ebz];
+                                tl[w++] = t;
+                            });
+    }
+}
+
+__global__ void __launch_bounds__(kHeavyEdgeBlock)
+    k_pe_fold_heavy(const int32_t* __restrict__ fwd, const int32_t* __restrict__ heavy_list,
+                    const unsigned* __restrict__ nheavy, const int64_t* __restrict__ tl_off,
+                    const TriEntry* __restrict__ tl, double* __restrict__ pe)
+{
+    __shared__ double s_w[kHeavyEdgeBlock / 32][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t nh = *nheavy;
+    const int64_t nwarps = (int64_t)gridDim.x * (kHeavyEdgeBlock / 32);
+    for (int64_t h = (int64_t)blockIdx.x * (kHeavyEdgeBlock / 32) + wib; h < nh; h += nwarps) {
+        const int64_t i = fwd[heavy_list[h]];
+        const int64_t e0 = tl_off[i], e1 = tl_off[i + 1];
+        double acc = 0.0;
+        for (int64_t b = e0; b < e1; b += 32) {
+            if (b + lane < e1) s_w[wib][lane] = tl[b + lane].wgt;
+            __syncwarp();
+            const int cnt = e1 - b < 32 ? (int)(e1 - b) : 32;
+            for (int j = 0; j < cnt; ++j) acc += s_w[wib][j];
+            __syncwarp();
+        }
+        if (lane == 0) pe[i] = acc;
     }
 }
 
@@ -266,7 +438,9 @@ int count_triangles(rtr_graph* g)
     Scratch sc(g);
     int64_t* cnt = (int64_t*)sc.get(sizeof(int64_t) * (m2 + 1));
     int64_t* tmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(m2 + 1));
-    if (!cnt || !tmp) {
+    int32_t* heavy_list = (int32_t*)sc.get(sizeof(int32_t) * (m + 1));
+    unsigned* nheavy = (unsigned*)sc.get(sizeof(unsigned) * 2);
+    if (!cnt || !tmp || !heavy_list || !nheavy) {
         set_error("device allocation failed (count scratch)");
         return RTR_ERR_CUDA;
     }
@@ -279,12 +453,16 @@ int count_triangles(rtr_graph* g)
     RTR_CUDA_TRY(cudaMemsetAsync(g->pe, 0, sizeof(double) * (m2 + 1), s));
     RTR_CUDA_TRY(cudaMemsetAsync(g->sup, 0, sizeof(uint32_t) * (m2 + 1), s));
     const int ge = grid_for(m, kBlock);
+    const int gh = grid_for(1ll << 40, kHeavyEdgeBlock, 16);
+    RTR_CUDA_TRY(cudaMemsetAsync(nheavy, 0, sizeof(unsigned), s));
     ktime_begin(g, KT_EDGE_FOLD);
     k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, m, g->pe, g->sup, cnt, g->ctr,
-                                      g->tune_gallop);
+                                      g->tune_gallop, g->tune_edge, heavy_list, nheavy);
+    k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->fwd, heavy_list, nheavy,
+                                                      g->tune_gallop, g->sup, cnt, g->ctr);
     ktime_end(g, KT_EDGE_FOLD);
     exclusive_scan_i64(cnt, g->tl_off, m2 + 1, nullptr, tmp, s);
-    g->launches += 4;
+    g->launches += 6;
     RTR_CUDA_TRY(cudaGetLastError());
     int64_t tl_len = 0;
     RTR_CUDA_TRY(cudaMemcpyAsync(&tl_len, g->tl_off + m2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -300,7 +478,10 @@ int count_triangles(rtr_graph* g)
     g->tl_len = tl_len;
     ktime_begin(g, KT_TRI_FILL);
     k_tri_fill<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd, g->frank, m,
-                                     g->tl_off, g->tl, g->tune_gallop);
+                                     g->tl_off, g->tl, g->tune_gallop, g->tune_edge);
+    k_tri_fill_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd,
+                                                    g->frank, heavy_list, nheavy, g->tune_gallop, g->tl_off, g->tl);
+    k_pe_fold_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->fwd, heavy_list, nheavy, g->tl_off, g->tl, g->pe);
     ktime_end(g, KT_TRI_FILL);
     ktime_begin(g, KT_VERTEX_FOLD);
     k_vertex_fold_light<<<grid_for(n, kBlock), kBlock, 0, s>>>(g->offsets, g->nbors, g->deg, g->partner, n,
@@ -308,7 +489,7 @@ int count_triangles(rtr_graph* g)
     k_vertex_fold_heavy<<<grid_for(1ll << 40, kHeavyBlock, 16), kHeavyBlock, 0, s>>>(
         g->offsets, g->nbors, g->deg, g->partner, n, g->tl_off, g->tl, g->pv, g->tune_heavy);
     ktime_end(g, KT_VERTEX_FOLD);
-    g->launches += 3;
+    g->launches += 5;
     RTR_CUDA_TRY(cudaGetLastError());
     cudaEventRecord(e1, s);
     RTR_CUDA_TRY(cudaEventSynchronize(e1));

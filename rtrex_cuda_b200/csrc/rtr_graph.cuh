@@ -75,7 +75,8 @@ struct rtr_graph {
     int stage = 0;
     // counting work split (results do not depend on it): gallop ratio and heavy-vertex degree
     int tune_gallop = 16;
-    int tune_heavy = 32;  // 1 built, 2 counted, 3 cleaned, 4 extracted
+    int tune_heavy = 32;
+    int tune_edge = 1024;  // deg u + deg v from which an edge is intersected by a warp  // 1 built, 2 counted, 3 cleaned, 4 extracted
 
     // stage timings from CUDA events (ms)
     float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0, ms_decompose = 0, ms_expand = 0;

@@ -138,7 +138,7 @@ def torch_cuda_available():
 
 def test_tuning_entry_points_argument_errors():
     L = rtr.lib()
-    a, b = ctypes.c_int(), ctypes.c_int()
-    assert L.rtr_set_tuning(None, 16, 32) == 1
-    assert L.rtr_get_tuning(None, ctypes.byref(a), ctypes.byref(b)) == 1
-    assert L.rtr_autotune(None, ctypes.byref(a), ctypes.byref(b)) == 1
+    a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    assert L.rtr_set_tuning(None, 16, 32, 1024) == 1
+    assert L.rtr_get_tuning(None, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)) == 1
+    assert L.rtr_autotune(None, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)) == 1

@@ -22,7 +22,7 @@ def _count(n, u, v, tuning=None):
 def test_every_work_split_gives_the_same_bits(name):
     n, u, v = helpers.case_graph(name)
     ref = _count(n, u, v)
-    for tuning in [(1, 1), (4, 8), (64, 128), (1 << 20, 1 << 30), (2, 2)]:
+    for tuning in [(1, 1, 1), (4, 8, 2), (64, 128, 64), (1 << 20, 1 << 30, 1 << 30), (2, 2, 16), (16, 32, 4)]:
         got = _count(n, u, v, tuning)
         for a, b in zip(got, ref):
             assert np.array_equal(a, b), (name, tuning)
@@ -31,9 +31,10 @@ def test_every_work_split_gives_the_same_bits(name):
 def test_autotune_then_decompose_matches_reference():
     (n, u, v), c, s0, s1, cl, _ = helpers.oracle_run("gnp_cliques", 0.3)
     with rtr.Graph.from_edges(n, u, v) as g:
-        gal, heavy = g.autotune()
+        gal, heavy, edge = g.autotune()
         assert gal in (4, 8, 16, 32, 64) and heavy in (8, 16, 32, 64, 128)
-        assert g.tuning() == (gal, heavy)
+        assert edge in (128, 256, 512, 1024, 4096, 1 << 30)
+        assert g.tuning() == (gal, heavy, edge)
         pe, pv, sup, t = g.weights()  # autotune leaves the graph counted
         assert t == s0.total and (helpers.bits(pe) == helpers.bits(s0.perEdge)).all()
         assert g.decompose(0.3) == len(cl)
