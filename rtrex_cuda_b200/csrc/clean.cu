@@ -25,6 +25,8 @@
 //    vertex's weight.  Lists longer than 32 entries are taken 64 at a time
 //    with the next window's entries fetched during the current window's
 //    records (pop_edge); shorter ones take the single-window path (pop_short).
+//    A window seed's first 32 entries are staged in shared memory by one TMA
+//    bulk copy per seed (cp.async.bulk, completing on a per-warp mbarrier).
 //    Entries are read evict-first (each list is read once), so streaming the
 //    lists does not displace the edge records from L2.  (Warming the next
 //    pop's lines with prefetch instructions was measured and costs more on
@@ -260,6 +262,7 @@ struct WarpSmem {
     TriEntry went[32][32];         // first 32 triangles of each seed in the window
     StackEntry wseed[32];          // the window's seeds (lane k = k-th seed in pop order)
     double sw[32];                 // per-lane triangle weights of the current chunk
+    uint64_t bar;                  // mbarrier completing the window's bulk copies
 };
 
 // Streaming read of a triangle-list entry: the clean reads each list once, so
@@ -273,14 +276,45 @@ __device__ __forceinline__ TriEntry ld_entry(const TriEntry* p)
     return t;
 }
 
-// Asynchronous 16-byte global -> shared copy (no register round trip); all of
-// a window's copies are issued back to back and waited for once.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+// Window staging by the TMA engine: one bulk global -> shared copy per seed
+// (its first <= 32 entries, a contiguous run of 32-byte entries: source,
+// destination and size are multiples of 16 bytes), all completing on the
+// warp's mbarrier, which lane 0 arms with the window's byte total.  No
+// multicast.  The wait is bounded.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar)
 {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arm(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_done(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+constexpr long kWaitLimit = 1l << 24;  // try_wait rounds before a wait is declared lost
 
 // Per-warp cascade stack: the newest entries in shared memory, older ones
 // spilled in order to the unit's global region (LIFO order is preserved).
@@ -524,6 +558,9 @@ __global__ void __launch_bounds__(kCleanBlock)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpSmem& sm = reinterpret_cast<WarpSmem*>(smem_raw)[wid];
     double* sw = sm.sw;
+    if (lane == 0) mbar_init(&sm.bar);
+    __syncwarp();
+    unsigned bar_phase = 0;
     while (true) {
         unsigned ui = 0;
         if (lane == 0) ui = atomicAdd(next_unit, 1u);
@@ -567,19 +604,27 @@ __global__ void __launch_bounds__(kCleanBlock)
                     }
                     wmask = __ballot_sync(0xffffffffu, live_seed);
                     sp = lo;
-                    // stage the first 32 triangles of every live seed (static data)
-                    for (unsigned mm = wmask; mm; mm &= mm - 1) {
-                        const int k = __ffs(mm) - 1;
-                        const int cnt = __shfl_sync(0xffffffffu, wseed.cnt, k);
-                        const int64_t t0 = __shfl_sync(0xffffffffu, wseed.t0, k);
-                        if (lane < cnt) {
-                            const char* src = reinterpret_cast<const char*>(a.tl + t0 + lane);
-                            char* dst = reinterpret_cast<char*>(&sm.went[k][lane]);
-                            cp_async16(dst, src);
-                            cp_async16(dst + 16, src + 16);
+                    // stage the first 32 triangles of every live seed (static data):
+                    // one bulk copy per seed, lane k copying seed k's run
+                    const unsigned bytes = live_seed ? 32u * (unsigned)(wseed.cnt < 32 ? wseed.cnt : 32) : 0u;
+                    const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
+                    if (total) {
+                        // earlier generic reads of the staging area precede the async writes
+                        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                        if (lane == 0) mbar_arm(&sm.bar, total);
+                        __syncwarp();
+                        if (bytes) bulk_to_smem(&sm.went[lane][0], a.tl + wseed.t0, bytes, &sm.bar);
+                        long it = 0;
+                        while (!mbar_done(&sm.bar, bar_phase) && ++it < kWaitLimit) {
                         }
+                        if (it >= kWaitLimit) {  // report, give the copies one more bounded wait, stop
+                            if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_WAIT);
+                            for (long j = 0; j < kWaitLimit && !mbar_done(&sm.bar, bar_phase); ++j) {
+                            }
+                            return;
+                        }
+                        bar_phase ^= 1u;
                     }
-                    cp_async_wait_all();
                     __syncwarp();
                     if (wmask == 0) continue;
                 }

@@ -69,6 +69,7 @@ enum DevErr : unsigned {
     DEV_ERR_BAD_STATUS = 1u << 1,
     DEV_ERR_SCRATCH = 1u << 2,
     DEV_ERR_SORT = 1u << 3,
+    DEV_ERR_WAIT = 1u << 4,  // a bounded wait on an asynchronous copy ran out
 };
 
 __host__ __device__ inline double tri_weight(int64_t a, int64_t b, int64_t c)
