@@ -430,17 +430,20 @@ __device__ __forceinline__ void pop_begin(const StackEntry& c, PopCtx& p)
     p.removed = 0;
 }
 
-// The popped edge's own state: lane 0 its support word, lanes 1-3 its weight
-// and its endpoints' weights (issued in the first round trip).
+// The popped edge's own state, one 8-byte load per lane (issued in the first
+// round trip): lane 0 the record's last word (list length | support word),
+// lane 1 its weight, lanes 2-3 its endpoints' weights.
 __device__ __forceinline__ void pop_own_loads(const CleanArgs& a, const StackEntry& c, uint32_t& s_e, double& scal)
 {
     const int lane = threadIdx.x & 31;
-    s_e = 0;
-    scal = 0.0;
-    if (lane == 0) s_e = a.rec[c.e].ss;
-    else if (lane == 1) scal = a.rec[c.e].pe;
-    else if (lane == 2) scal = a.pv[c.first];
-    else if (lane == 3) scal = a.pv[c.second];
+    const EdgeRec* r = a.rec + c.e;
+    const unsigned long long* src =
+        lane == 0 ? reinterpret_cast<const unsigned long long*>(&r->cnt)
+        : lane == 1 ? reinterpret_cast<const unsigned long long*>(&r->pe)
+        : reinterpret_cast<const unsigned long long*>(a.pv + (lane == 2 ? c.first : c.second));
+    const unsigned long long w = lane < 4 ? *src : 0ull;
+    s_e = (uint32_t)(w >> 32);  // meaningful on lane 0 (ss follows cnt)
+    scal = __longlong_as_double((long long)w);
 }
 
 // False when the edge has no live triangle left (it is retired here).
