@@ -430,31 +430,33 @@ __device__ __forceinline__ void pop_begin(const StackEntry& c, PopCtx& p)
     p.removed = 0;
 }
 
-// The popped edge's own state, one 8-byte load per lane (issued in the first
-// round trip): lane 0 the record's last word (list length | support word),
-// lane 1 its weight, lanes 2-3 its endpoints' weights.
-__device__ __forceinline__ void pop_own_loads(const CleanArgs& a, const StackEntry& c, uint32_t& s_e, double& scal)
+// The popped edge's own state, loaded by every lane from warp-uniform addresses
+// (broadcast loads, no shuffles): the record's last word (list length |
+// support word), its weight and its endpoints' weights.  Issued in the first
+// round trip.
+struct OwnState {
+    unsigned long long w;  // cnt | ss << 32
+    double pe, pu, pv;
+};
+
+__device__ __forceinline__ void pop_own_loads(const CleanArgs& a, const StackEntry& c, OwnState& o)
 {
-    const int lane = threadIdx.x & 31;
     const EdgeRec* r = a.rec + c.e;
-    const unsigned long long* src =
-        lane == 0 ? reinterpret_cast<const unsigned long long*>(&r->cnt)
-        : lane == 1 ? reinterpret_cast<const unsigned long long*>(&r->pe)
-        : reinterpret_cast<const unsigned long long*>(a.pv + (lane == 2 ? c.first : c.second));
-    const unsigned long long w = lane < 4 ? *src : 0ull;
-    s_e = (uint32_t)(w >> 32);  // meaningful on lane 0 (ss follows cnt)
-    scal = __longlong_as_double((long long)w);
+    o.w = *reinterpret_cast<const unsigned long long*>(&r->cnt);
+    o.pe = r->pe;
+    o.pu = a.pv[c.first];
+    o.pv = a.pv[c.second];
 }
 
 // False when the edge has no live triangle left (it is retired here).
-__device__ __forceinline__ bool pop_own_state(const CleanArgs& a, const StackEntry& c, uint32_t& s_e, double scal,
-                                              PopCtx& p, unsigned long long* diag)
+__device__ __forceinline__ bool pop_own_state(const CleanArgs& a, const StackEntry& c, const OwnState& o,
+                                              uint32_t& s_e, PopCtx& p, unsigned long long* diag)
 {
     const int lane = threadIdx.x & 31;
-    s_e = __shfl_sync(0xffffffffu, s_e, 0) & SS_SUP;
-    p.acc_e = __shfl_sync(0xffffffffu, scal, 1);
-    p.acc_u = __shfl_sync(0xffffffffu, scal, 2);
-    p.acc_v = __shfl_sync(0xffffffffu, scal, 3);
+    s_e = (uint32_t)(o.w >> 32) & SS_SUP;
+    p.acc_e = o.pe;
+    p.acc_u = o.pu;
+    p.acc_v = o.pv;
     if (s_e == 0) {
         if (lane == 0) {
             if (fabs(p.acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
@@ -493,14 +495,14 @@ __device__ __forceinline__ int pop_short(const CleanArgs& a, const StackEntry& c
     PopCtx p;
     pop_begin(c, p);
     uint32_t s_e;
-    double scal;
-    pop_own_loads(a, c, s_e, scal);
+    OwnState own;
+    pop_own_loads(a, c, own);
     Group g;
     g.valid = lane < c.cnt;
     g.t = TriEntry{};
     if (g.valid) g.t = staged ? staged[lane] : ld_entry(a.tl + c.t0 + lane);
     if (staged) load_group(a, g, p.lower_is_a);
-    if (!pop_own_state(a, c, s_e, scal, p, diag)) return 0;
+    if (!pop_own_state(a, c, own, s_e, p, diag)) return 0;
     if (!staged) load_group(a, g, p.lower_is_a);
     if (!apply_group(a, g, p, ws, sw, err)) return -1;
     pop_end(a, c, s_e, p, diag);
@@ -519,8 +521,8 @@ __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c,
     PopCtx p;
     pop_begin(c, p);
     uint32_t s_e;
-    double scal;
-    pop_own_loads(a, c, s_e, scal);
+    OwnState own;
+    pop_own_loads(a, c, own);
     Group g0, g1;
     g0.valid = lane < c.cnt;
     g1.valid = 32 + lane < c.cnt;
@@ -530,7 +532,7 @@ __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c,
     if (g1.valid) g1.t = ld_entry(a.tl + c.t0 + 32 + lane);
     const bool seed_records = staged != nullptr;
     if (seed_records) load_group(a, g0, p.lower_is_a);
-    if (!pop_own_state(a, c, s_e, scal, p, diag)) return 0;
+    if (!pop_own_state(a, c, own, s_e, p, diag)) return 0;
     TriEntry n0{}, n1{};
     for (int base = 0; base < c.cnt; base += 64) {
         if (base > 0) {
