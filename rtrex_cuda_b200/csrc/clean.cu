@@ -471,13 +471,12 @@ __device__ __forceinline__ bool pop_own_state(const CleanArgs& a, const StackEnt
 __device__ __forceinline__ void pop_end(const CleanArgs& a, const StackEntry& c, uint32_t s_e, const PopCtx& p,
                                         unsigned long long* diag)
 {
-    if ((threadIdx.x & 31) == 0) {
-        a.rec[c.e].pe = p.acc_e;
-        a.rec[c.e].ss = (s_e - (uint32_t)p.removed) | SS_N;
-        a.pv[c.first] = p.acc_u;
-        a.pv[c.second] = p.acc_v;
-        if (fabs(p.acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
-    }
+    // every lane holds the same values: the same stores from all lanes, no branch
+    a.rec[c.e].pe = p.acc_e;
+    a.rec[c.e].ss = (s_e - (uint32_t)p.removed) | SS_N;
+    a.pv[c.first] = p.acc_u;
+    a.pv[c.second] = p.acc_v;
+    if ((threadIdx.x & 31) == 0 && fabs(p.acc_e) > a.inv_n) atomicAdd(&diag[0], 1ull);
     __syncwarp();
 }
 

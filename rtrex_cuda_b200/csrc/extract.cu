@@ -269,22 +269,31 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
             if (valid) t = a.tl[p];
             const int32_t elw = lower_is_a ? t.eaz : t.ebz;
             const int32_t ehw = lower_is_a ? t.ebz : t.eaz;
+            // statuses, weights and supports of the triangle's other cells in one
+            // round trip (the weights are only used when the triangle is live)
             uint8_t slw = ST_N, shw = ST_N;
+            double pel = 0.0, peh = 0.0, pz = 0.0;
+            uint32_t sul = 0, suh = 0;
             if (valid) {
                 slw = a.st[elw];
                 shw = a.st[ehw];
+                pel = a.pe[elw];
+                peh = a.pe[ehw];
+                pz = a.pv[t.z];
+                sul = a.sup[elw];
+                suh = a.sup[ehw];
             }
             const bool live = valid && slw != ST_N && shw != ST_N;
             const double wgt = live ? t.wgt : 0.0;
             bool q1 = false, q2 = false;
             if (live) {
-                const double x1 = a.pe[elw] - wgt;
-                const double x2 = a.pe[ehw] - wgt;
+                const double x1 = pel - wgt;
+                const double x2 = peh - wgt;
                 a.pe[elw] = x1;
                 a.pe[ehw] = x2;
-                a.pv[t.z] -= wgt;
-                a.sup[elw] -= 1u;
-                a.sup[ehw] -= 1u;
+                a.pv[t.z] = pz - wgt;
+                a.sup[elw] = sul - 1u;
+                a.sup[ehw] = suh - 1u;
                 q1 = slw != ST_S && x1 < a.eps * (1 / (double)(dlow * (int64_t)t.dz));
                 q2 = shw != ST_S && x2 < a.eps * (1 / (double)(dhigh * (int64_t)t.dz));
             }
@@ -322,14 +331,13 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
             __syncwarp();
         }
         if (overflow) return;
-        if (lane == 0) {
-            a.pe[e] = acc_e;
-            a.pv[u] = acc_u;
-            a.pv[v] = acc_v;
-            a.sup[e] = s_e - rem;
-            if (fabs(acc_e) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
-            a.st[e] = ST_N;
-        }
+        // every lane holds the same values: the same stores from all lanes, no branch
+        a.pe[e] = acc_e;
+        a.pv[u] = acc_u;
+        a.pv[v] = acc_v;
+        a.sup[e] = s_e - rem;
+        a.st[e] = ST_N;
+        if (lane == 0 && fabs(acc_e) > a.inv_n) atomicAdd(&a.diag[0], 1ull);
         removed += rem;
     }
     __syncwarp();
@@ -493,7 +501,8 @@ __global__ void __launch_bounds__(kExtractBlock) k_extract_components(ExtractArg
                 }
             }
             int fail = 0;
-            int64_t ntop = 0;  // deletion stack built by lane 0, replayed by the warp
+            int64_t ntop = 0;         // deletion stack size, built and replayed by the warp
+            int32_t ncl_members = 0;  // size of the cluster just cut out (lane 0)
             if (lane == 0) {
                 sort_ids(twohop, n2);
                 double potential = 0;
@@ -537,29 +546,52 @@ __global__ void __launch_bounds__(kExtractBlock) k_extract_components(ExtractArg
                     a.hdr_seed[vb + ncl] = u;
                     a.hdr_start[vb + ncl] = out;
                     a.hdr_size[vb + ncl] = S.size;
+                    ncl_members = S.size;
                     for (int32_t p = S.head; p != -1; p = S.next[p]) a.out_vert[out++] = S.key[p] + base;
                     ++ncl;
-
-                    int64_t top = 0;
-                    for (int32_t p = S.head; p != -1; p = S.next[p]) {
-                        const int32_t z = S.key[p] + base;
-                        for (int64_t j = a.off[z]; j < a.off[z + 1]; ++j) {
-                            const int64_t f = fwd_slot(z, j, a.nb, a.partner);
-                            if (a.st[f] != ST_Y) continue;
-                            if (top >= cd.scap) {
-                                atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
-                                break;
-                            }
-                            dstack[top++] = DelEntry{(int32_t)f, z, a.nb[j], 0};
-                            a.st[f] = ST_S;
-                        }
-                    }
-                    ntop = top;
                 }
             }
             __syncwarp();
             if (__shfl_sync(0xffffffffu, fail, 0)) break;
-            delete_and_clean_warp(a, dstack, __shfl_sync(0xffffffffu, ntop, 0), cd.scap, sw);
+            // The deletion stack: every still-'Y' edge of the cluster's members, members
+            // in set-iteration order (the list lane 0 just wrote to out_vert) and each
+            // member's row in order, 32 row entries at a time.  An edge between two
+            // members is pushed from the first member's row only ('S' afterwards).
+            {
+                const int32_t nm = __shfl_sync(0xffffffffu, ncl_members, 0);
+                const int64_t mbase = __shfl_sync(0xffffffffu, out, 0) - nm;
+                int64_t top = 0;
+                bool full = false;
+                for (int32_t q = 0; q < nm && !full; ++q) {
+                    const int32_t z = a.out_vert[mbase + q];
+                    const int64_t j1 = a.off[z + 1];
+                    for (int64_t jb = a.off[z]; jb < j1; jb += 32) {
+                        const int64_t j = jb + lane;
+                        int64_t f = -1;
+                        bool push = false;
+                        if (j < j1) {
+                            f = fwd_slot(z, j, a.nb, a.partner);
+                            push = a.st[f] == ST_Y;
+                        }
+                        const unsigned pm = __ballot_sync(0xffffffffu, push);
+                        const int np = __popc(pm);
+                        if (top + np > cd.scap) {
+                            if (lane == 0) atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                            full = true;  // stop scanning; the cascade still runs on what was pushed
+                            break;
+                        }
+                        if (push) {
+                            dstack[top + __popc(pm & lt)] = DelEntry{(int32_t)f, z, a.nb[j], 0};
+                            a.st[f] = ST_S;
+                        }
+                        top += np;
+                        __syncwarp();
+                    }
+                }
+                ntop = top;
+            }
+            __syncwarp();
+            delete_and_clean_warp(a, dstack, ntop, cd.scap, sw);
         }
         if (lane == 0) a.ncl[c] = ncl;
     }
