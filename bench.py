@@ -163,6 +163,37 @@ def replica_max(x: float, world: int, device) -> float:
     return float(t.item())
 
 
+def shard(items, rank: int, world: int):
+    """Rank `rank`'s share of independent work items (graphs, requests): every
+    world-th item, so sizes drawn from one distribution spread evenly."""
+    return list(items)[rank::world] if world > 1 else list(items)
+
+
+def gather_values(vals, world: int):
+    """Concatenate every rank's list of values (all ranks receive the result)."""
+    if world <= 1:
+        return list(vals)
+    import torch.distributed as dist
+    parts = [None] * world
+    dist.all_gather_object(parts, list(vals))
+    return [x for part in parts for x in part]
+
+
+def dist_init():
+    """(world, rank, local device) under torchrun; NCCL only for barriers and
+    the max / gather of timings -- no collective is on the data path."""
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
 def replica_value(edges_per_rank: int, world: int, ms_step: float) -> float:
     """Whole-job edges/s: every rank decomposes its own copy in ms_step (max over ranks)."""
     return world * edges_per_rank / (ms_step / 1e3)
@@ -401,13 +432,14 @@ def batch_arm(args):
     import torch
     import rtrex_cuda_b200 as rtr
     from rtrex_cuda_b200 import graphgen
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
+    world, rank, dev = dist_init()
+    allmax = lambda x: replica_max(x, world, torch.device("cuda", dev))
     t0 = time.perf_counter()
-    graphs = graphgen.sbm_batch(args.batch_graphs)
+    all_graphs = graphgen.sbm_batch(args.batch_graphs)
     gen_s = time.perf_counter() - t0
-    K = len(graphs)
-    edges = int(sum(g[1].size for g in graphs))
+    K = len(all_graphs)
+    edges = int(sum(g[1].size for g in all_graphs))
+    graphs = shard(all_graphs, rank, world)  # independent graphs: every rank its own share
     # the counting work split is chosen by the autotuner on the first batch
     # (untimed) and reused for every later batch
     with rtr.Graph.batch(graphs, device=dev) as g:
@@ -424,21 +456,24 @@ def batch_arm(args):
         t1 = time.perf_counter()
         if k >= args.warmup:
             times.append(t1 - t0)
-    batched_s = float(np.mean(times))
-    dev_s = float(np.mean(dev_ms[args.warmup:])) / 1e3
+    batched_s = allmax(float(np.mean(times)))
+    dev_s = allmax(float(np.mean(dev_ms[args.warmup:])) / 1e3)
     # plain leg: one graph at a time, one pass (warmed by the batched leg)
     t0 = time.perf_counter()
     plain_counts = []
     for (n, u, v) in graphs:
         with rtr.Graph.from_edges(n, u, v, device=dev) as g1:
             plain_counts.append(g1.decompose(args.eps))
-    plain_s = time.perf_counter() - t0
-    same = bool((np.asarray(plain_counts) == counts).all())
+    plain_s = allmax(time.perf_counter() - t0)
+    same = bool(all(gather_values([bool((np.asarray(plain_counts) == counts).all())], world)))
+    if rank != 0:
+        return
     line = {
         "metric": "batched graphs/s (count+clean+extract)", "value": K / dev_s, "unit": "graphs/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_s * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "sbm_batch", "graphs": K, "edges": edges, "eps": args.eps,
+                   "parallelism": f"graphs sharded over {world} GPU(s), every {world}th graph per rank",
                    "desc": "SBM graphs, 4-64 blocks, intra mean degree 12, inter 2, edge targets log-uniform "
                            "in [1K, 200K], seeds 4000+i; disjoint union decomposed in one call",
                    "autotune": {"gallop_ratio": tuning[0], "heavy_degree": tuning[1], "heavy_edge": tuning[2]}},
@@ -463,15 +498,20 @@ def serve_arm(args):
     import torch
     import rtrex_cuda_b200 as rtr
     from rtrex_cuda_b200 import graphgen
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
+    world, rank, dev = dist_init()
+    allmax = lambda x: replica_max(x, world, torch.device("cuda", dev))
     t0 = time.perf_counter()
     pool = graphgen.served_pool(args.serve_pool, m_hi=args.serve_max_edges)
     gen_s = time.perf_counter() - t0
     rng = np.random.default_rng(6000)
     N = args.serve_requests
-    req_graph = rng.integers(0, len(pool), size=N)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=N))
+    all_graph = rng.integers(0, len(pool), size=N)
+    all_arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=N))
+    # independent requests: rank r serves every world-th request of the stream,
+    # at that request's own arrival time
+    mine = shard(range(N), rank, world)
+    req_graph = all_graph[mine]
+    arrivals = all_arrivals[mine]
     eps = args.eps
     digest = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.int64).tobytes()).hexdigest()
     # plain leg (also the reference results): each request alone, in order
@@ -491,7 +531,7 @@ def serve_arm(args):
             cof = g.cluster_of()
         plain_lat.append(time.perf_counter() - t1)
         plain.setdefault(gid, (tri, left, k, digest(cof)))
-    plain_s = time.perf_counter() - t0
+    plain_s = allmax(time.perf_counter() - t0)
     # served leg
     with rtr.Server(device=dev, hbm_budget=int(args.serve_budget_gb * (1 << 30)), workers=args.serve_workers,
                     batch_max_edges=20000, batch_max_graphs=64) as srv:
@@ -506,18 +546,25 @@ def serve_arm(args):
             rids.append(srv.submit(gid, eps))
         res = [srv.wait(r) for r in rids]
         st = srv.stats()
-    lat = np.array([r["t_end_ms"] - r["t_submit_ms"] for r in res])
-    service = np.array([r["t_end_ms"] - r["t_start_ms"] for r in res])
-    span_ms = max(r["t_end_ms"] for r in res) - min(r["t_submit_ms"] for r in res)
-    bad = sum(1 for r, gid in zip(res, req_graph.tolist())
-              if r["status"] != 0 or (r["triangles"], r["triangles_left"], r["n_clusters"], digest(r["cluster_of"]))
-              != plain[gid])
-    edges = int(sum(pool[g][1].size for g in req_graph.tolist()))
+    # every rank's latencies pooled; the job's span is the slowest rank's
+    lat = np.array(gather_values([r["t_end_ms"] - r["t_submit_ms"] for r in res], world))
+    service = np.array(gather_values([r["t_end_ms"] - r["t_start_ms"] for r in res], world))
+    span_ms = allmax(max(r["t_end_ms"] for r in res) - min(r["t_submit_ms"] for r in res) if res else 0.0)
+    plain_lat = gather_values(plain_lat, world)
+    bad = sum(gather_values([sum(1 for r, gid in zip(res, req_graph.tolist())
+                                 if r["status"] != 0 or (r["triangles"], r["triangles_left"], r["n_clusters"],
+                                                         digest(r["cluster_of"])) != plain[gid])], world))
+    every_st = gather_values([st], world)
+    st = {k: sum(d[k] for d in every_st) for k in st}
+    edges = int(sum(pool[g][1].size for g in all_graph.tolist()))
+    if rank != 0:
+        return
     line = {
         "metric": "served p99 latency (ms)", "value": float(np.percentile(lat, 99)), "unit": "ms",
-        "n_gpus": 1, "steps": N, "warmup": 2, "ms_per_step": float(span_ms / N), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "n_gpus": world, "steps": N, "warmup": 2, "ms_per_step": float(span_ms / N), "higher_is_better": False,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "served", "requests": N, "arrival_rate_per_s": args.serve_rate,
+                   "parallelism": f"requests sharded over {world} GPU(s), every {world}th request per rank",
                    "pool_graphs": len(pool), "edge_range": [1000, args.serve_max_edges], "eps": eps,
                    "workers": args.serve_workers, "hbm_budget_gb": args.serve_budget_gb,
                    "batch_max_edges": 20000, "batch_max_graphs": 64,
@@ -537,11 +584,11 @@ def serve_arm(args):
 
 def main():
     args = parse_args()
-    if args.workload == "batch":
-        batch_arm(args)
-        return
-    if args.workload == "serve":
-        serve_arm(args)
+    if args.workload in ("batch", "serve"):
+        (batch_arm if args.workload == "batch" else serve_arm)(args)
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
         return
     if args.impl == "reference":
         reference_arm(args)
