@@ -106,6 +106,16 @@ int rtr_get_memory(const rtr_graph* g, int64_t* resident_bytes, int64_t* peak_sc
 int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree, int heavy_edge);
 int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int* heavy_edge);
 
+/* Split of the cascading clean: units (connected components of the
+ * triangle-carrying edges) with at least min_seeds seeds and triangle lists of
+ * at most max_mean_list entries on average are replayed in parallel rounds by
+ * one thread block each -- pops whose cells are disjoint run together,
+ * perVertex is folded afterwards in the reference's pop order -- and the other
+ * units one warp per unit.  Defaults 2048 and 8.  Results are the same bits
+ * for every setting.  No counterpart in the reference. */
+int rtr_set_clean_split(rtr_graph* g, int64_t min_seeds, double max_mean_list);
+int rtr_get_clean_split(const rtr_graph* g, int64_t* min_seeds, double* max_mean_list);
+
 /* Autotuner: times the counting pass on this graph for gallop ratios
  * {4,8,16,32,64}, then heavy degrees {8,16,32,64,128}, then heavy-edge degree
  * sums {128,256,512,1024,4096,off} (coordinate descent, each candidate timed by

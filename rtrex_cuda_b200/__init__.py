@@ -104,6 +104,8 @@ def lib():
     L.rtr_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.rtr_get_tuning.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rtr_autotune.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rtr_set_clean_split.argtypes = [_vp, _i64, ctypes.c_double]
+    L.rtr_get_clean_split.argtypes = [_vp, P(_i64), P(ctypes.c_double)]
     L.rtr_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, _i64, ctypes.c_int, P(_vp)]
     L.rtr_server_add_graph.argtypes = [_vp, _vp, _vp, _i64, _i64, ctypes.c_int, P(_i64)]
     L.rtr_server_submit.argtypes = [_vp, _i64, ctypes.c_double, _vp, P(_i64)]
@@ -323,6 +325,17 @@ class Graph:
     def set_tuning(self, gallop_ratio: int, heavy_degree: int, heavy_edge: int = 1024):
         """Counting work split (results are identical for every setting)."""
         _check(lib().rtr_set_tuning(self._h, int(gallop_ratio), int(heavy_degree), int(heavy_edge)))
+
+    def set_clean_split(self, min_seeds: int, max_mean_list: float = 8.0):
+        """Clean units with at least `min_seeds` seeds and triangle lists of at
+        most `max_mean_list` entries on average replay in parallel rounds (one
+        thread block each), the others one warp per unit (same bits)."""
+        _check(lib().rtr_set_clean_split(self._h, int(min_seeds), float(max_mean_list)))
+
+    def clean_split(self):
+        v, x = _i64(), ctypes.c_double()
+        _check(lib().rtr_get_clean_split(self._h, ctypes.byref(v), ctypes.byref(x)))
+        return int(v.value), float(x.value)
 
     def tuning(self):
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

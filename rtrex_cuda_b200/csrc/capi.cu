@@ -343,6 +343,7 @@ int rtr_graph_destroy(rtr_graph* g)
     for (int k = 0; k < 2 * rtr_graph::kTimers; ++k)
         if (g->kev[k]) cudaEventDestroy(g->kev[k]);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+    if (g->side) cudaStreamDestroy(g->side);
     delete[] g->batch_vbase;
     delete g;
     return RTR_OK;
@@ -357,6 +358,28 @@ int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree, int heavy_e
     g->tune_gallop = gallop_ratio;
     g->tune_heavy = heavy_degree;
     g->tune_edge = heavy_edge;
+    return RTR_OK;
+}
+
+int rtr_set_clean_split(rtr_graph* g, int64_t min_seeds, double max_mean_list)
+{
+    if (!g || min_seeds < 1 || !(max_mean_list >= 0)) {
+        set_error("rtr_set_clean_split: null graph, min_seeds below 1 or max_mean_list negative");
+        return RTR_ERR_ARG;
+    }
+    g->clean_round_min = min_seeds;
+    g->clean_round_list = max_mean_list;
+    return RTR_OK;
+}
+
+int rtr_get_clean_split(const rtr_graph* g, int64_t* min_seeds, double* max_mean_list)
+{
+    if (!g || !min_seeds || !max_mean_list) {
+        set_error("rtr_get_clean_split: null argument");
+        return RTR_ERR_ARG;
+    }
+    *min_seeds = g->clean_round_min;
+    *max_mean_list = g->clean_round_list;
     return RTR_OK;
 }
 

@@ -37,6 +37,7 @@
 //    the reference's push order (triangle order, (lower,w) before (higher,w)).
 //    Seeds are loaded 32 at a time; support only decreases, so a seed whose
 //    support is already 0 when loaded is retired without a pop.
+#include "clean_units.cuh"
 #include "primitives.cuh"
 #include "rtr_graph.cuh"
 
@@ -154,14 +155,19 @@ __global__ void k_uf_flatten(int32_t* __restrict__ p, int64_t n)
         p[v] = uf_find(p, (int32_t)v);
 }
 
-// Per-unit capacity of the cascade stack: the unit's triangle-carrying edges.
+// Per-unit capacity of the cascade stack (the unit's triangle-carrying edges)
+// and the total length of their triangle lists.
 __global__ void k_unit_edges(const int32_t* __restrict__ esrc, const int32_t* __restrict__ fwd, int64_t m,
                              const uint32_t* __restrict__ sup, const int32_t* __restrict__ root,
-                             uint32_t* __restrict__ ecount)
+                             uint32_t* __restrict__ ecount, unsigned long long* __restrict__ tsum)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = fwd[k];
-        if (sup[i] > 0) atomicAdd(&ecount[root[esrc[i]]], 1u);
+        if (sup[i] > 0) {
+            const int32_t r = root[esrc[i]];
+            atomicAdd(&ecount[r], 1u);
+            atomicAdd(&tsum[r], (unsigned long long)sup[i]);
+        }
     }
 }
 
@@ -181,13 +187,6 @@ __global__ void k_unit_heads(const uint64_t* __restrict__ keys, int64_t ns, int 
         head[j] = (j == 0 || (keys[j] >> rbits) != (keys[j - 1] >> rbits)) ? 1u : 0u;
 }
 
-struct UnitDesc {
-    int64_t seed_begin;
-    int64_t seed_end;
-    int64_t stack_base;
-    int64_t stack_cap;
-};
-
 __global__ void k_unit_desc(const uint64_t* __restrict__ keys, int64_t ns, int rbits,
                             const uint32_t* __restrict__ head, const uint32_t* __restrict__ hpos,
                             const uint32_t* __restrict__ ecount, UnitDesc* __restrict__ units,
@@ -197,38 +196,33 @@ __global__ void k_unit_desc(const uint64_t* __restrict__ keys, int64_t ns, int r
         if (!head[j]) continue;
         const uint32_t u = hpos[j];
         units[u].seed_begin = j;
+        units[u].root = (int64_t)(keys[j] >> rbits);
         cap[u] = ecount[(uint32_t)(keys[j] >> rbits)];
     }
 }
 
+// Unit bounds and the schedule: the units replayed in parallel rounds (many
+// seeds, short lists: those are where disjoint pops are common) first, then
+// the others; within each group the units with the most seeds first.
 __global__ void k_unit_finish(UnitDesc* __restrict__ units, const int64_t* __restrict__ cap,
                               const int64_t* __restrict__ capoff, int64_t nu, int64_t ns,
-                              uint64_t* __restrict__ order_keys)
+                              const uint32_t* __restrict__ ecount, const unsigned long long* __restrict__ tsum,
+                              int64_t round_min, double round_max_list, uint64_t* __restrict__ order_keys,
+                              unsigned* __restrict__ nbig)
 {
     for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < nu; u += (int64_t)gridDim.x * blockDim.x) {
         units[u].seed_end = (u + 1 < nu) ? units[u + 1].seed_begin : ns;
         units[u].stack_base = capoff[u];
         units[u].stack_cap = cap[u];
-        // schedule units with the most seeds first
         const uint64_t work = (uint64_t)(units[u].seed_end - units[u].seed_begin);
-        order_keys[u] = ((uint64_t)(0xffffffffu - (uint32_t)(work < 0xffffffffull ? work : 0xffffffffull)) << 32) |
+        const int64_t r = units[u].root;
+        const bool rounds = (int64_t)work >= round_min && (double)tsum[r] <= round_max_list * (double)ecount[r];
+        if (rounds) atomicAdd(nbig, 1u);
+        order_keys[u] = ((uint64_t)(rounds ? 0u : 1u) << 63) |
+                        ((uint64_t)(0x7fffffffu - (uint32_t)(work < 0x7fffffffull ? work : 0x7fffffffull)) << 32) |
                         (uint64_t)u;
     }
 }
-
-// One cascade-stack entry: the pair as deleteAndClean pushed it plus the
-// static data its pop needs (degrees, triangle-list bounds), so a pop issues
-// no lookups before its first dynamic load.  Seeds use the same descriptor.
-struct StackEntry {
-    int32_t e;        // forward rank of the edge
-    int32_t first;    // Pair.first  (deleteAndClean's u)
-    int32_t second;   // Pair.second (deleteAndClean's v)
-    int32_t dfirst;   // deg(first)
-    int32_t dsecond;  // deg(second)
-    int32_t cnt;      // triangle-list length
-    int64_t t0;       // triangle-list start
-};
-static_assert(sizeof(StackEntry) == 32, "StackEntry is 32 bytes");
 
 // Seed descriptors, sorted seed j (unit-major, slot order within a unit).
 __global__ void k_seed_info(const uint64_t* __restrict__ keys, int64_t ns, uint64_t rmask,
@@ -264,17 +258,6 @@ struct WarpSmem {
     double sw[32];                 // per-lane triangle weights of the current chunk
     uint64_t bar;                  // mbarrier completing the window's bulk copies
 };
-
-// Streaming read of a triangle-list entry: the clean reads each list once, so
-// entries are loaded evict-first and do not displace the edge records in L2.
-__device__ __forceinline__ TriEntry ld_entry(const TriEntry* p)
-{
-    TriEntry t;
-    int4* d = reinterpret_cast<int4*>(&t);
-    d[0] = __ldcs(reinterpret_cast<const int4*>(p));
-    d[1] = __ldcs(reinterpret_cast<const int4*>(p) + 1);
-    return t;
-}
 
 // Window staging by the TMA engine: one bulk global -> shared copy per seed
 // (its first <= 32 entries, a contiguous run of 32-byte entries: source,
@@ -554,9 +537,10 @@ __device__ __forceinline__ int pop_edge(const CleanArgs& a, const StackEntry& c,
 }
 
 __global__ void __launch_bounds__(kCleanBlock)
-    k_clean_units(CleanArgs a, const UnitDesc* __restrict__ units, const uint64_t* __restrict__ order, int64_t nu,
-                  StackEntry* __restrict__ stacks, unsigned* __restrict__ next_unit, unsigned* __restrict__ err,
-                  unsigned long long* __restrict__ total, unsigned long long* __restrict__ diag)
+    k_clean_units(CleanArgs a, const UnitDesc* __restrict__ units, const uint64_t* __restrict__ order, int64_t first,
+                  int64_t nu, StackEntry* __restrict__ stacks, unsigned* __restrict__ next_unit,
+                  unsigned* __restrict__ err, unsigned long long* __restrict__ total,
+                  unsigned long long* __restrict__ diag)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -569,8 +553,8 @@ __global__ void __launch_bounds__(kCleanBlock)
         unsigned ui = 0;
         if (lane == 0) ui = atomicAdd(next_unit, 1u);
         ui = __shfl_sync(0xffffffffu, ui, 0);
-        if ((int64_t)ui >= nu) break;
-        const UnitDesc ud = units[(uint32_t)order[ui]];
+        if (first + (int64_t)ui >= nu) break;
+        const UnitDesc ud = units[(uint32_t)order[first + ui]];
         WarpStack ws{sm.stack, stacks + ud.stack_base, 0, ud.stack_cap, 0};
         int64_t sp = ud.seed_end;  // seeds [seed_begin, sp) not yet loaded
         // Window of the next 32 seeds in pop order (lane k = seed sp_at_load-1-k).
@@ -647,6 +631,14 @@ __global__ void __launch_bounds__(kCleanBlock)
     }
 }
 
+struct SideWait {
+    cudaStream_t st = nullptr;
+    ~SideWait()
+    {
+        if (st) cudaStreamSynchronize(st);
+    }
+};
+
 }  // namespace
 
 int initial_clean(rtr_graph* g, double eps)
@@ -670,8 +662,9 @@ int initial_clean(rtr_graph* g, double eps)
     uint32_t* d_ns = (uint32_t*)sc.get(sizeof(uint32_t) * 2);
     int32_t* root = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
     uint32_t* ecount = (uint32_t*)sc.get(sizeof(uint32_t) * (n + 1));
+    unsigned long long* tsum = (unsigned long long*)sc.get(sizeof(unsigned long long) * (n + 1));
     EdgeRec* rec = (EdgeRec*)sc.get(sizeof(EdgeRec) * (m + 1));
-    if (!is_seed || !spos || !stmp || !d_ns || !root || !ecount || !rec) {
+    if (!is_seed || !spos || !stmp || !d_ns || !root || !ecount || !tsum || !rec) {
         set_error("device allocation failed (clean)");
         return RTR_ERR_CUDA;
     }
@@ -684,7 +677,8 @@ int initial_clean(rtr_graph* g, double eps)
     k_uf_hook_support<<<gm, kBlock, 0, s>>>(g->esrc, g->nbors, g->fwd, m, g->sup, root);
     k_uf_flatten<<<gn, kBlock, 0, s>>>(root, n);
     RTR_CUDA_TRY(cudaMemsetAsync(ecount, 0, sizeof(uint32_t) * (n + 1), s));
-    k_unit_edges<<<gm, kBlock, 0, s>>>(g->esrc, g->fwd, m, g->sup, root, ecount);
+    RTR_CUDA_TRY(cudaMemsetAsync(tsum, 0, sizeof(unsigned long long) * (n + 1), s));
+    k_unit_edges<<<gm, kBlock, 0, s>>>(g->esrc, g->fwd, m, g->sup, root, ecount, tsum);
     exclusive_scan_u32(is_seed, spos, m, d_ns, stmp, s);
     g->launches += 8;
     RTR_CUDA_TRY(cudaGetLastError());
@@ -728,38 +722,64 @@ int initial_clean(rtr_graph* g, double eps)
         uint64_t* okeys = (uint64_t*)sc.get(sizeof(uint64_t) * (nu + 1));
         uint64_t* oalt = (uint64_t*)sc.get(sizeof(uint64_t) * (nu + 1));
         void* otmp = sc.get(radix_temp_bytes(nu));
-        unsigned* next_unit = (unsigned*)sc.get(sizeof(unsigned) * 2);
+        unsigned* next_unit = (unsigned*)sc.get(sizeof(unsigned) * 4);
         if (!units || !cap || !capoff || !ctmp || !d_cap_total || !okeys || !oalt || !otmp || !next_unit) {
             set_error("device allocation failed (clean units)");
             return RTR_ERR_CUDA;
         }
+        RTR_CUDA_TRY(cudaMemsetAsync(next_unit, 0, sizeof(unsigned) * 4, s));
         k_unit_desc<<<gs, kBlock, 0, s>>>(sorted, ns, rbits, head, hpos, ecount, units, cap);
         exclusive_scan_i64(cap, capoff, nu, d_cap_total, ctmp, s);
-        k_unit_finish<<<grid_for(nu, kBlock), kBlock, 0, s>>>(units, cap, capoff, nu, ns, okeys);
+        k_unit_finish<<<grid_for(nu, kBlock), kBlock, 0, s>>>(units, cap, capoff, nu, ns, ecount, tsum,
+                                                              g->clean_round_min, g->clean_round_list, okeys,
+                                                              next_unit + 1);
         uint64_t* order = radix_sort_u64(okeys, oalt, nu, 64, otmp, s);
         g->launches += 5 + 24;
         int64_t cap_total = 0;
+        unsigned nbig = 0;
         RTR_CUDA_TRY(cudaMemcpyAsync(&cap_total, d_cap_total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        RTR_CUDA_TRY(cudaMemsetAsync(next_unit, 0, sizeof(unsigned) * 2, s));
+        RTR_CUDA_TRY(cudaMemcpyAsync(&nbig, next_unit + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         RTR_CUDA_TRY(cudaStreamSynchronize(s));
         StackEntry* stacks = (StackEntry*)sc.get(sizeof(StackEntry) * (cap_total + 1));
         if (!stacks) {
             set_error("device allocation failed (clean stacks)");
             return RTR_ERR_CUDA;
         }
-        CleanArgs ca{g->tl, rec, g->pv, 1 / (double)n, seeds};
-        // one warp per unit, persistent over the unit list (largest units first)
-        int blocks = (int)std::min<int64_t>((nu + kCleanWarps - 1) / kCleanWarps,
-                                            (int64_t)grid_for(1 << 30, kCleanBlock, 8));
-        blocks = std::max(blocks, 1);
         ktime_begin(g, KT_CLEAN_UNITS);
-        const size_t smem = sizeof(WarpSmem) * kCleanWarps;
-        RTR_CUDA_TRY(cudaFuncSetAttribute(k_clean_units, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_clean_units<<<blocks, kCleanBlock, smem, s>>>(ca, units, order, nu, stacks, next_unit,
-                                                        (unsigned*)(g->ctr + 1), g->ctr, g->ctr + 2);
+        // the largest units (order[0, nbig)) replay in parallel rounds on the
+        // side stream while the others replay one warp per unit here
+        RoundReplay rr;
+        cudaEvent_t joined = nullptr;
+        SideWait side_wait;  // an early return waits for the side stream before scratch is freed
+        if (nbig > 0) {
+            if (!g->side) RTR_CUDA_TRY(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking));
+            side_wait.st = g->side;
+            const int rc = clean_rounds_launch(g, sc, g->side, rec, seeds, units, order, nbig, stacks, &rr);
+            if (rc) return rc;
+            RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
+            RTR_CUDA_TRY(cudaEventRecord(joined, g->side));
+        }
+        if ((int64_t)nbig < (int64_t)nu) {
+            CleanArgs ca{g->tl, rec, g->pv, 1 / (double)n, seeds};
+            // one warp per unit, persistent over the unit list (largest units first)
+            const int64_t nsmall = (int64_t)nu - (int64_t)nbig;
+            int blocks = (int)std::min<int64_t>((nsmall + kCleanWarps - 1) / kCleanWarps,
+                                                (int64_t)grid_for(1 << 30, kCleanBlock, 8));
+            blocks = std::max(blocks, 1);
+            const size_t smem = sizeof(WarpSmem) * kCleanWarps;
+            RTR_CUDA_TRY(cudaFuncSetAttribute(k_clean_units, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_clean_units<<<blocks, kCleanBlock, smem, s>>>(ca, units, order, (int64_t)nbig, nu, stacks, next_unit,
+                                                            (unsigned*)(g->ctr + 1), g->ctr, g->ctr + 2);
+            g->launches += 1;
+            RTR_CUDA_TRY(cudaGetLastError());
+        }
+        if (nbig > 0) {
+            RTR_CUDA_TRY(cudaStreamWaitEvent(s, joined, 0));
+            cudaEventDestroy(joined);
+            const int rc = clean_rounds_finish(g, sc, &rr);
+            if (rc) return rc;
+        }
         ktime_end(g, KT_CLEAN_UNITS);
-        g->launches += 1;
-        RTR_CUDA_TRY(cudaGetLastError());
     }
     k_clean_finish<<<gm, kBlock, 0, s>>>(g->fwd, m, rec, g->pe, g->sup, g->st);
     g->launches += 1;

@@ -72,11 +72,17 @@ struct rtr_graph {
     int64_t* batch_vbase = nullptr;  // host copy, [nbatch+1]
 
     double eps = 0.3;
-    int stage = 0;
+    int stage = 0;  // 1 built, 2 counted, 3 cleaned, 4 extracted
     // counting work split (results do not depend on it): gallop ratio and heavy-vertex degree
     int tune_gallop = 16;
     int tune_heavy = 32;
-    int tune_edge = 1024;  // deg u + deg v from which an edge is intersected by a warp  // 1 built, 2 counted, 3 cleaned, 4 extracted
+    int tune_edge = 1024;  // deg u + deg v from which an edge is intersected by a warp
+    // clean units with at least this many seeds and triangle lists of at most
+    // this mean length replay in parallel rounds (one thread block each); the
+    // others one warp per unit
+    int64_t clean_round_min = 2048;
+    double clean_round_list = 8.0;
+    cudaStream_t side = nullptr;  // second stream of the graph (created on first use)
 
     // stage timings from CUDA events (ms)
     float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0, ms_decompose = 0, ms_expand = 0;

@@ -142,3 +142,10 @@ def test_tuning_entry_points_argument_errors():
     assert L.rtr_set_tuning(None, 16, 32, 1024) == 1
     assert L.rtr_get_tuning(None, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)) == 1
     assert L.rtr_autotune(None, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)) == 1
+
+
+def test_clean_split_entry_points_argument_errors():
+    L = rtr.lib()
+    k, x = ctypes.c_int64(), ctypes.c_double()
+    assert L.rtr_set_clean_split(None, 2048, 8.0) == 1
+    assert L.rtr_get_clean_split(None, ctypes.byref(k), ctypes.byref(x)) == 1
