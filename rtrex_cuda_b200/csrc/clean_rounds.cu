@@ -115,6 +115,37 @@ __device__ __forceinline__ int h_insert(RoundSmem& S, unsigned cell, unsigned ow
     return -1;
 }
 
+// Claims of one triangle's two other edges, both probes issued before either
+// is resolved (the edges differ).
+__device__ __forceinline__ void h_insert2(RoundSmem& S, unsigned c1, unsigned c2, unsigned owner, double w, int& s1,
+                                          int& s2)
+{
+    unsigned a = (c1 * 2654435761u) >> (32 - kHashBits), b = (c2 * 2654435761u) >> (32 - kHashBits);
+    unsigned ka = atomicCAS(&S.hkey[a], kNoCell, c1);
+    unsigned kb = atomicCAS(&S.hkey[b], kNoCell, c2);
+    s1 = s2 = -1;
+    for (int probe = 0; probe < kHashSlots; ++probe) {
+        if (ka == kNoCell || ka == c1) {
+            s1 = (int)a;
+            break;
+        }
+        a = (a + 1) & (kHashSlots - 1);
+        ka = atomicCAS(&S.hkey[a], kNoCell, c1);
+    }
+    for (int probe = 0; probe < kHashSlots; ++probe) {
+        if (kb == kNoCell || kb == c2) {
+            s2 = (int)b;
+            break;
+        }
+        b = (b + 1) & (kHashSlots - 1);
+        kb = atomicCAS(&S.hkey[b], kNoCell, c2);
+    }
+    if (s1 >= 0) atomicMin(&S.hown[s1], owner);
+    if (s2 >= 0) atomicMin(&S.hown[s2], owner);
+    if (s1 >= 0) atomicAdd(&S.hacc[s1], w);
+    if (s2 >= 0) atomicAdd(&S.hacc[s2], w);
+}
+
 __device__ __forceinline__ void h_clear(RoundSmem& S, int slot)
 {
     if (slot >= 0) {
@@ -394,19 +425,17 @@ __global__ void __launch_bounds__(kRoundBlock, 1) k_clean_rounds(RoundArgs a)
         }
         const uint32_t c1 = r1.ss & SS_CODE, c2 = r2.ss & SS_CODE;
         const bool live = valid && c1 != SS_N && c2 != SS_N;
-        // ---- reserve
+        // ---- reserve (the own cell by the first lane without a triangle, lane 31 for a full list)
+        const int ol = c.cnt < 32 ? c.cnt : 31;
         int so = -1, s1 = -1, s2 = -1;
-        if (active && !lng && lane == 0) so = h_insert(S, (unsigned)c.e, (unsigned)wid, 0.0, false);
-        if (live) {
-            s1 = h_insert(S, (unsigned)rlw, (unsigned)wid, t.wgt, true);
-            s2 = h_insert(S, (unsigned)rhw, (unsigned)wid, t.wgt, true);
-        }
+        if (active && !lng && lane == ol) so = h_insert(S, (unsigned)c.e, (unsigned)wid, 0.0, false);
+        if (live) h_insert2(S, (unsigned)rlw, (unsigned)rhw, (unsigned)wid, t.wgt, s1, s2);
         __syncthreads();
         // ---- decide
         RoundCtl& ctl = S.ctl[par];
         if (tid == 0) S.ctl[par ^ 1] = RoundCtl{kRoundWarps, kRoundWarps, 0, 0u};
         bool mine = !lng, may = lng;
-        if (active && !lng && lane == 0) mine = so >= 0 && S.hown[so] == (unsigned)wid;
+        if (active && !lng && lane == ol) mine = so >= 0 && S.hown[so] == (unsigned)wid;
         if (live) mine = mine && s1 >= 0 && s2 >= 0 && S.hown[s1] == (unsigned)wid && S.hown[s2] == (unsigned)wid;
         const bool winner = __all_sync(kFull, mine) && active;
         double x1 = 0.0, x2 = 0.0, acc_e = ope;
@@ -443,7 +472,7 @@ __global__ void __launch_bounds__(kRoundBlock, 1) k_clean_rounds(RoundArgs a)
                     }
                 }
             }
-            if (lane == 0 && !lng && so < 0) may = true;
+            if (lane == ol && !lng && so < 0) may = true;
             if (__any_sync(kFull, may) && lane == 0) atomicMin(&ctl.cut, wid);
         }
         __syncthreads();
