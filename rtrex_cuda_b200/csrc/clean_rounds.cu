@@ -78,6 +78,7 @@ struct RoundSmem {
     double hacc[kHashSlots];         // sum of the claiming triangles' weights
     double sw[kRoundWarps][32];      // per-warp live weights, packed in triangle order
     RoundCtl ctl[2];
+    int wcnt[kRoundWarps];           // per-warp counts of a refill's kept seeds
     int np_solo;                     // pend count after a solo pop
     long long gtop_solo;
     int stop;
@@ -322,20 +323,48 @@ __global__ void __launch_bounds__(kRoundBlock, 1) k_clean_rounds(RoundArgs a)
         {
             const int nU = __popc(U);
             const int T = nU + npush;  // items in front of pend
-            if (np < kRoundWarps && (gtop > 0 || sp > ud.seed_begin)) {
+            while (np < kRoundWarps && (gtop > 0 || sp > ud.seed_begin)) {
                 // refill pend from below: the global region first, then the seeds
-                const bool from_gm = gtop > 0;
-                const int k = (int)(from_gm ? (gtop < kRefill ? gtop : kRefill)
-                                            : (sp - ud.seed_begin < kRefill ? sp - ud.seed_begin : kRefill));
                 StackEntry keep{};
                 if (tid < np) keep = S.pend[tid];
-                __syncthreads();
-                if (tid < np) S.pend[k + tid] = keep;
-                for (int j = tid; j < k; j += kRoundBlock)
-                    S.pend[j] = from_gm ? gm[gtop - k + j] : a.seeds[sp - k + j];
-                if (from_gm) gtop -= k;
-                else sp -= k;
-                np += k;
+                if (gtop > 0) {
+                    const int k = (int)(gtop < kRefill ? gtop : kRefill);
+                    __syncthreads();
+                    if (tid < np) S.pend[k + tid] = keep;
+                    for (int j = tid; j < k; j += kRoundBlock) S.pend[j] = gm[gtop - k + j];
+                    gtop -= k;
+                    np += k;
+                } else {
+                    // Seeds whose support is already 0 are retired here without a
+                    // pop (support only decreases; such a pop touches no cell but
+                    // its own and pushes nothing) and take no window slot.
+                    static_assert(kRefill <= kRoundBlock, "one refill candidate per thread");
+                    const int k = (int)(sp - ud.seed_begin < kRefill ? sp - ud.seed_begin : kRefill);
+                    StackEntry se{};
+                    bool kept = false;
+                    if (tid < k) {
+                        se = a.seeds[sp - k + tid];
+                        const EdgeRec* r = a.rec + se.e;
+                        kept = (r->ss & SS_SUP) > 0;
+                        if (!kept) {
+                            if (fabs(r->pe) > a.inv_n) atomicAdd(a.diag, 1ull);
+                            a.rec[se.e].ss = SS_N;
+                        }
+                    }
+                    const unsigned bal = __ballot_sync(kFull, kept);
+                    if (lane == 0) S.wcnt[wid] = __popc(bal);
+                    __syncthreads();
+                    int below = 0, kk = 0;
+                    for (int w = 0; w < kRoundWarps; ++w) {
+                        const int cw = S.wcnt[w];
+                        below += w < wid ? cw : 0;
+                        kk += cw;
+                    }
+                    if (tid < np) S.pend[kk + tid] = keep;
+                    if (kept) S.pend[below + __popc(bal & lt)] = se;  // seed order kept
+                    sp -= k;
+                    np += kk;
+                }
                 __syncthreads();
             }
             const int avail = T + np;
