@@ -7,8 +7,10 @@ each would touch (its own edge and the two other edges of every live
 triangle); a pop that owns all its cells is a winner; winners commit in one
 round unless an earlier item is a winner that pushes (its pushes are spliced in
 right after it) or a loser that might push (some live-triangle edge could fall
-below threshold after every claim of the window); seeds whose support is already
-0 when they are loaded into the pending list are retired without a pop.
+below threshold after every claim of the window); an item whose list is longer
+than the kernel's 32 entries is popped alone at the front of the window and
+elsewhere ends the commits before it; seeds whose support is already 0 when
+they are loaded into the pending list are retired without a pop.
 perVertex is not touched during the rounds: each pop's subtractions are logged
 and replayed afterwards in the reference's pop order, recovered from a linked
 sequence list.  If the policy were unsound, some perEdge / perVertex bit or
@@ -37,7 +39,7 @@ def _graph(seed):
     return n, su, sv
 
 
-def _round_replay(n, u, v, eps, W, refill, loser_cut=True):
+def _round_replay(n, u, v, eps, W, refill, loser_cut=True, long_list=32):
     c = oracle.build_csr(n, u, v)
     s0 = oracle.count(c)
     off, nb = c.offsets, c.nbors
@@ -101,16 +103,23 @@ def _round_replay(n, u, v, eps, W, refill, loser_cut=True):
             pend = kept + pend
         if not pend:
             break
-        win = [pend.pop() for _ in range(min(W, len(pend)))]
+        # an item with a list longer than long_list is popped alone at the front;
+        # elsewhere it claims no cell and nothing after it commits
+        width = 1 if len(tris(pend[-1][0])) > long_list else W
+        win = [pend.pop() for _ in range(min(width, len(pend)))]
+        lng = [i > 0 and len(tris(e)) > long_list for i, (e, _) in enumerate(win)]
         owner, acc, claims = {}, {}, []
         for i, (e, pr) in enumerate(win):
-            cl = [(e, 0.0)] + [(x, w) for (lw, hw, z, w) in live(e, pr) for x in (lw, hw)]
+            cl = [] if lng[i] else [(e, 0.0)] + [(x, w) for (lw, hw, z, w) in live(e, pr) for x in (lw, hw)]
             claims.append(cl)
             for x, w in cl:
                 owner.setdefault(x, i)
                 acc[x] = acc.get(x, 0.0) + w
         cut, p1, pushes, results = len(win), None, [], {}
         for i, (e, pr) in enumerate(win):
+            if lng[i]:
+                cut = min(cut, i)
+                continue
             if all(owner[x] == i for x, _ in claims[i]):  # winner: exact on round-start values
                 u_, v_ = pr
                 du, dv = int(deg[u_]), int(deg[v_])
@@ -185,11 +194,13 @@ def _round_replay(n, u, v, eps, W, refill, loser_cut=True):
 
 
 @pytest.mark.parametrize("seed", range(12))
-@pytest.mark.parametrize("W,refill", [(16, 512), (4, 3)])
-def test_round_policy_matches_sequential_replay(seed, W, refill):
+@pytest.mark.parametrize("W,refill,long_list", [(16, 512, 32), (4, 3, 32), (16, 64, 2)])
+def test_round_policy_matches_sequential_replay(seed, W, refill, long_list):
+    """long_list=2 makes most items "long": popped alone at the front, ending the
+    commits elsewhere (the kernel's path for lists over 32 entries)."""
     n, u, v = _graph(seed)
     eps = [0.3, 0.1, 0.5][seed % 3]
-    c, s0, P, S, T, PV = _round_replay(n, u, v, eps, W, refill)
+    c, s0, P, S, T, PV = _round_replay(n, u, v, eps, W, refill, long_list=long_list)
     s1 = oracle.initial_clean(c, s0, eps)
     fwd = np.repeat(np.arange(n), np.diff(c.offsets)) < c.nbors
     assert (T[fwd] == s1.status[fwd]).all()
