@@ -26,7 +26,7 @@ import numpy as np
 
 __all__ = [
     "simplify", "gnp_cliques", "chung_lu", "rmat", "sbm", "small_test",
-    "write_escape", "read_escape", "config_graph",
+    "write_escape", "read_escape", "parse_escape", "config_graph",
 ]
 
 
@@ -237,9 +237,20 @@ def write_escape(path: str, n: int, u: np.ndarray, v: np.ndarray) -> None:
 
 
 def read_escape(path: str):
-    """Parse an Escape file into ``(n, u, v)`` (lines in file order, no simplification)."""
-    with open(path, "rb") as f:
-        data = f.read()
+    """Parse an Escape file (plain or gzip-compressed, ``.gz``) into ``(n, u, v)``
+    (lines in file order, no simplification)."""
+    if path.endswith(".gz"):
+        import gzip
+        with gzip.open(path, "rb") as f:
+            data = f.read()
+    else:
+        with open(path, "rb") as f:
+            data = f.read()
+    return parse_escape(data)
+
+
+def parse_escape(data: bytes):
+    """Parse Escape edge-list bytes into ``(n, u, v)`` (lines in order, no simplification)."""
     lines = [ln for ln in data.split(b"\n") if ln.strip() and not ln.startswith(b"#")]
     head = lines[0].split()
     n, m = int(head[0]), int(head[1])

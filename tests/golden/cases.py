@@ -2,8 +2,10 @@
 
 Every case is either regenerated from a seed by rtrex_cuda_b200.graphgen, built
 by hand below (edge cases), or one of the reference's bundled data files
-(BUNDLED; read from the reference checkout, so those cases only run where it
-is present).  CASES maps a case name to the thresholds it is checked at; 0.3 is
+(BUNDLED: RTRex_Sequential/clustering/{random_graph_rtr,clean_email,clean_astro}.txt,
+kept byte for byte, gzip-compressed, under tests/golden/data/ so they run
+wherever the tests run; tests/golden/make_golden.py --copy-bundled refreshes them
+from a reference checkout).  CASES maps a case name to the thresholds it is checked at; 0.3 is
 the reference's documented setting (RTRex_CUDA/README.md) and 0.1 the paper's.
 
 The SBM cases at eps=0.1 are order-sensitive: a bulk-synchronous peel leaves a
@@ -16,11 +18,21 @@ import numpy as np
 
 from rtrex_cuda_b200 import graphgen
 
+import os
+
+# bundled case -> its file inside the reference project
 BUNDLED = {
     "random_graph_rtr": "RTRex_Sequential/clustering/random_graph_rtr.txt",
     "clean_email": "RTRex_Sequential/clustering/clean_email.txt",
     "clean_astro": "RTRex_Sequential/clustering/clean_astro.txt",
 }
+
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+def bundled_path(name: str) -> str:
+    """The committed (gzip) copy of a bundled case's data file."""
+    return os.path.join(DATA_DIR, os.path.basename(BUNDLED[name]) + ".gz")
 
 CASES = {
     # edge cases
@@ -84,7 +96,9 @@ def _clique(vs):
 
 
 def load_case(name: str):
-    """(n, src, dst) for a case that does not come from a bundled file."""
+    """(n, src, dst) for a fixture case (bundled files in file-line order)."""
+    if name in BUNDLED:
+        return graphgen.read_escape(bundled_path(name))
     if name == "isolated":
         return _pairs(5, [])
     if name == "no_edges_but_one":

@@ -18,14 +18,17 @@ graph and records, per stage, the reference's results:
 small_test (the reference's RTRex_Sequential/Example/small-test.txt graph)
 additionally stores full arrays in small_test.npz.  Graph inputs are either
 regenerated from seeds (rtrex_cuda_b200.graphgen) or, for the bundled data
-files, read from the reference checkout (those cases skip when it is absent).
+files, the committed copies under tests/golden/data/ (``--copy-bundled``
+refreshes those copies, byte for byte, from the reference checkout first).
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference] [--expand-only]
-(--expand-only recomputes only the expand entries of an existing golden.json)
+Usage: python tests/golden/make_golden.py [--reference DIR] [--copy-bundled] [--expand-only]
+(DIR defaults to $RTR_REFERENCE_DIR, else /root/reference; --expand-only
+recomputes only the expand entries of an existing golden.json)
 """
 from __future__ import annotations
 
 import argparse
+import gzip
 import hashlib
 import json
 import os
@@ -40,7 +43,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from rtrex_cuda_b200 import graphgen  # noqa: E402
-from tests.golden.cases import CASES, BUNDLED, EXPAND, load_case  # noqa: E402
+from tests.golden.cases import CASES, BUNDLED, EXPAND, bundled_path, load_case  # noqa: E402
 
 
 def sha(b: bytes) -> str:
@@ -112,10 +115,29 @@ def run_reference_expand(dump_bin: str, cli_bin: str, path: str, eps: float, thr
     return out
 
 
+def bundled_text(name, td):
+    """Decompress the committed copy of a bundled file to td (the reference reads plain text)."""
+    path = os.path.join(td, os.path.basename(BUNDLED[name]))
+    with gzip.open(bundled_path(name), "rb") as f, open(path, "wb") as g:
+        g.write(f.read())
+    return path
+
+
+def copy_bundled(reference):
+    """Refresh tests/golden/data/ from the reference's own data files (gzip -9, no name/time stamp)."""
+    os.makedirs(os.path.dirname(bundled_path(next(iter(BUNDLED)))), exist_ok=True)
+    for name, rel in BUNDLED.items():
+        with open(os.path.join(reference, rel), "rb") as f:
+            data = f.read()
+        with open(bundled_path(name), "wb") as raw:
+            with gzip.GzipFile(filename="", mode="wb", compresslevel=9, fileobj=raw, mtime=0) as g:
+                g.write(data)
+        print("copied", rel, len(data), "bytes")
+
+
 def case_path(name, td, reference):
     if name in BUNDLED:
-        path = os.path.join(reference, BUNDLED[name])
-        return path if os.path.exists(path) else None
+        return bundled_text(name, td)
     n, u, v = load_case(name)
     path = os.path.join(td, name + ".txt")
     graphgen.write_escape(path, n, u, v)
@@ -136,9 +158,12 @@ def add_expand(golden, dump_bin, cli_bin, reference):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("RTR_REFERENCE_DIR", "/root/reference"))
+    ap.add_argument("--copy-bundled", action="store_true")
     ap.add_argument("--expand-only", action="store_true")
     args = ap.parse_args()
+    if args.copy_bundled:
+        copy_bundled(args.reference)
     dump_bin = os.path.join(ROOT, "oracle", "_ref", "rtr_ref_dump")
     cli_bin = os.path.join(ROOT, "oracle", "_ref", "RTRex")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.reference}"], check=True)
@@ -153,10 +178,7 @@ def main():
     with tempfile.TemporaryDirectory() as td:
         for name, eps_list in CASES.items():
             if name in BUNDLED:
-                path = os.path.join(args.reference, BUNDLED[name])
-                if not os.path.exists(path):
-                    print("skip", name)
-                    continue
+                path = bundled_text(name, td)
             else:
                 n, u, v = load_case(name)
                 path = os.path.join(td, name + ".txt")

@@ -12,14 +12,12 @@ import json
 import os
 
 import numpy as np
-import pytest
 
 import oracle
-from tests.golden.cases import BUNDLED, load_case
+from tests.golden.cases import load_case
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden", "golden.json")
-REFERENCE = os.environ.get("RTR_REFERENCE_DIR", "/root/reference")
 
 
 def sha(b: bytes) -> str:
@@ -33,13 +31,7 @@ def golden():
 
 
 def case_graph(name: str):
-    """(n, src, dst) for a fixture case; skips bundled cases without the data file."""
-    if name in BUNDLED:
-        path = os.path.join(REFERENCE, BUNDLED[name])
-        if not os.path.exists(path):
-            pytest.skip(f"{BUNDLED[name]} is only available beside the reference checkout")
-        from rtrex_cuda_b200 import graphgen
-        return graphgen.read_escape(path)
+    """(n, src, dst) for a fixture case (the bundled reference files are committed copies)."""
     return load_case(name)
 
 
