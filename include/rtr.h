@@ -64,6 +64,18 @@ const char* rtr_last_error(void);
 int rtr_graph_create_from_edges(const int64_t* src, const int64_t* dst, int64_t m, int64_t n, int device, int flags,
                                 rtr_graph** out);
 
+/* Build an R-MAT graph on `device` without host edge arrays: 2^scale vertices,
+ * edge_factor * 2^scale generated pairs (below 2^30) with quadrant
+ * probabilities a, b, c (d = 1-a-b-c), symmetrised, self-loops and repeated
+ * pairs dropped.  Edge k's bit at level l comes from the splitmix64 output
+ * function of seed * 0x9E3779B97F4A7C15 ^ (k << 6 | l): high 32 bits >=
+ * floor((a+b) 2^32) sets the source bit, low 32 bits >= floor(a/(a+b) 2^32)
+ * (source bit clear) or floor(c/(1-a-b) 2^32) (set) the destination bit, level
+ * l giving bit scale-1-l.  For synthetic large-graph workloads; no counterpart
+ * in the reference, which reads edge-list files. */
+int rtr_graph_create_rmat(int scale, int64_t edge_factor, double a, double b, double c, uint64_t seed, int device,
+                          rtr_graph** out);
+
 /* Build a graph from a host CSR (symmetric, rows strictly ascending).
  * Replaces: transferGraphToDevice(h_offsets, h_nbors, nVertices, nEdges, dg)
  *           (RTRex_CUDA/gpu_graph.cuh:47-52) with allocateDeviceState (:57). */
@@ -106,6 +118,20 @@ int rtr_get_memory(const rtr_graph* g, int64_t* resident_bytes, int64_t* peak_sc
 int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree, int heavy_edge);
 int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int* heavy_edge);
 
+/* Counting layout.  mode 0 (the default) keeps the per-edge triangle lists
+ * (32 B per triangle and edge) when they fit in the device memory that is free
+ * beside what the clean needs, and otherwise counts without them; mode 1 always
+ * keeps them (RTR_ERR_CUDA when they do not fit); mode 2 never does.  Without
+ * lists ("rows layout") perVertex and the perEdge of heavy edges are folded
+ * straight from the CSR rows -- the same bits -- and vertices of at least
+ * hub_degree neighbours (default 4096) are folded by a whole thread block; the
+ * clean and the extraction need the lists, so rtr_clean then returns
+ * RTR_ERR_LIMIT.  *lists_kept tells whether the last rtr_count kept them.  No
+ * counterpart in the reference, whose commonNbr keeps no lists
+ * (RTRex_Sequential/Escape/Decomposition.h:42-117). */
+int rtr_set_count_mode(rtr_graph* g, int mode, int hub_degree);
+int rtr_get_count_mode(const rtr_graph* g, int* mode, int* hub_degree, int* lists_kept);
+
 /* Split of the cascading clean: units (connected components of the
  * triangle-carrying edges) with at least min_seeds seeds and triangle lists of
  * at most max_mean_list entries on average are replayed in parallel rounds by
@@ -115,6 +141,16 @@ int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int
  * for every setting.  No counterpart in the reference. */
 int rtr_set_clean_split(rtr_graph* g, int64_t min_seeds, double max_mean_list);
 int rtr_get_clean_split(const rtr_graph* g, int64_t* min_seeds, double* max_mean_list);
+
+/* Bounds of the clean's device-side self-checks, to test their error reports
+ * (no counterpart in the reference).  first_wait_rounds limits the first
+ * bounded wait of the warp-per-unit replay on each window's asynchronous copies
+ * (0 = the full limit); when it runs out the warp reports it and drains the
+ * copies under the full limit before it stops.  stack_entries caps every unit's
+ * cascade-stack region (-1 = sized to the unit).  A check that fires makes
+ * rtr_clean return RTR_ERR_DEVICE with the condition named in rtr_last_error();
+ * the graph's results are then incomplete but the device stays usable. */
+int rtr_set_clean_checks(rtr_graph* g, int64_t first_wait_rounds, int64_t stack_entries);
 
 /* Autotuner: times the counting pass on this graph for gallop ratios
  * {4,8,16,32,64}, then heavy degrees {8,16,32,64,128}, then heavy-edge degree
@@ -205,17 +241,23 @@ int rtr_get_kernel_ms(const rtr_graph* g, double* ms, int n);
  * from its own arena, or a latency-critical path where cudaMalloc/cudaFree may
  * synchronise the device).  No counterpart in the reference: it is an extra
  * entry point of this library.
- *   d_offsets int64[n+1], d_nbors int32[2m]  symmetric CSR on the current device,
- *                                            rows strictly ascending
+ *   d_offsets int64[n+1], d_nbors int32[2m]  symmetric CSR on the current device:
+ *                                            offsets non-decreasing from 0 to 2m,
+ *                                            rows strictly ascending, ids in [0, n),
+ *                                            no self-loops
  *   d_perEdge f64[2m], d_perVertex f64[n], d_support u32[2m], d_total int64[1]
  *                                            outputs, bit-identical to rtr_count's
  *   stream    a cudaStream_t (NULL = the default stream); the call is
  *             asynchronous and the outputs are ready when the stream is
- * Working memory is one fixed static device array (about 4.2 MB, held by every
+ * Every buffer must be non-null when n > 0 (RTR_ERR_ARG otherwise).  Neighbour
+ * ids outside [0, n) are skipped, never dereferenced, and make *d_total -1.
+ * Working memory is one fixed static device array (about 4.3 MB, held by every
  * GPU that loads librtr.so until exit), so n is limited to 1,048,576 vertices;
  * larger graphs get RTR_ERR_LIMIT.  The first call on each device looks up that
- * array's device address (make it before any stream capture).  All calls share
- * the array, so calls that overlap on the GPU race: serialise them. */
+ * array's device address (make it before any stream capture; a failed lookup is
+ * retried by the next call, and the address is not valid after a
+ * cudaDeviceReset).  All calls share the array, so calls that overlap on the
+ * GPU race: serialise them. */
 int rtr_count_noalloc(const int64_t* d_offsets, const int32_t* d_nbors, int64_t n, double* d_perEdge,
                       double* d_perVertex, uint32_t* d_support, int64_t* d_total, void* stream);
 

@@ -57,6 +57,12 @@ def lib():
         L.orc_expand.argtypes = [_i64, _i64p, _i64p, _i64, _i64p, _i64p, _i64p, _i64p, _i64p,
                                  ctypes.POINTER(_i64), _i64p, _f64p]
         L.orc_expand.restype = _i64
+        L.orc_cells_edge.argtypes = [_i64, _i64p, _i64p, _i64, _i64p, _f64p, _u32p]
+        L.orc_cells_edge.restype = None
+        L.orc_cells_vertex.argtypes = [_i64, _i64p, _i64p, _i64, _i64p, _f64p]
+        L.orc_cells_vertex.restype = None
+        L.orc_count_total.argtypes = [_i64, _i64p, _i64p]
+        L.orc_count_total.restype = _i64
         L.orc_selfcheck_counts.argtypes = [ctypes.POINTER(_i64)] * 3
         L.orc_selfcheck_reset.argtypes = []
         _lib = L
@@ -216,3 +222,34 @@ def run(n: int, u: np.ndarray, v: np.ndarray, eps: float):
     s1 = initial_clean(c, s0, eps)
     cl, s2 = extract(c, s1, eps)
     return c, s0, s1, cl, s2
+
+
+def cells_edge(offsets: np.ndarray, nbors: np.ndarray, slots) -> tuple[np.ndarray, np.ndarray]:
+    """perEdge and support of the sampled directed slots, recomputed from the CSR
+    alone (commonNbr's left fold over the common neighbours in ascending order)."""
+    offsets = np.ascontiguousarray(offsets, np.int64)
+    nbors = np.ascontiguousarray(nbors, np.int64) if len(nbors) else np.zeros(1, np.int64)
+    slots = np.ascontiguousarray(slots, np.int64)
+    pe = np.zeros(max(1, slots.size), np.float64)
+    sup = np.zeros(max(1, slots.size), np.uint32)
+    if slots.size:
+        lib().orc_cells_edge(offsets.size - 1, offsets, nbors, slots.size, slots, pe, sup)
+    return pe[:slots.size], sup[:slots.size]
+
+
+def cells_vertex(offsets: np.ndarray, nbors: np.ndarray, verts) -> np.ndarray:
+    """perVertex of the sampled vertices, recomputed from the CSR alone."""
+    offsets = np.ascontiguousarray(offsets, np.int64)
+    nbors = np.ascontiguousarray(nbors, np.int64) if len(nbors) else np.zeros(1, np.int64)
+    verts = np.ascontiguousarray(verts, np.int64)
+    pv = np.zeros(max(1, verts.size), np.float64)
+    if verts.size:
+        lib().orc_cells_vertex(offsets.size - 1, offsets, nbors, verts.size, verts, pv)
+    return pv[:verts.size]
+
+
+def count_total(offsets: np.ndarray, nbors: np.ndarray) -> int:
+    """Number of triangles of the CSR (degree-oriented count, independent of the folds)."""
+    offsets = np.ascontiguousarray(offsets, np.int64)
+    nbors = np.ascontiguousarray(nbors, np.int64) if len(nbors) else np.zeros(1, np.int64)
+    return int(lib().orc_count_total(offsets.size - 1, offsets, nbors))

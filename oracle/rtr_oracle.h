@@ -12,6 +12,7 @@
  *   orc_initial_clean  initialClean (mode s)     Decomposition.h:302-460 (+ deleteAndClean :147-283)
  *   orc_extract        disjointExtract loop      Decomposition.h:566-919 (+ populateStats :473-491)
  *   orc_expand         expandClusters            Decomposition.h:958-1008
+ *   orc_cells_*        commonNbr, cell by cell   Decomposition.h:70-115 (rtr_cells.cpp)
  *
  * Status bytes use the reference's characters: 'Y' alive, 'S' on the
  * deletion stack, 'N' deleted.  support[] is an integer companion the
@@ -65,6 +66,16 @@ int64_t orc_extract(int64_t n, const int64_t* offsets, const int64_t* nbors, con
 int64_t orc_expand(int64_t n, const int64_t* offsets, const int64_t* nbors, int64_t threshold,
                    int64_t* cl_nv, int64_t* cl_ne, int64_t* cl_cut, int64_t* cl_off, int64_t* cl_vert,
                    int64_t* n_scores, int64_t* sc_vertex, double* sc_value);
+
+/* Per-cell restatement of commonNbr's folds (rtr_cells.cpp), for graphs too
+ * large for orc_count: perEdge and support of the k directed slots slots[],
+ * perVertex of the k vertices verts[] (outputs indexed like the samples), and
+ * the triangle total.  Multi-threaded (OpenMP). */
+void orc_cells_edge(int64_t n, const int64_t* offsets, const int64_t* nbors, int64_t k, const int64_t* slots,
+                    double* perEdge, uint32_t* support);
+void orc_cells_vertex(int64_t n, const int64_t* offsets, const int64_t* nbors, int64_t k, const int64_t* verts,
+                      double* perVertex);
+int64_t orc_count_total(int64_t n, const int64_t* offsets, const int64_t* nbors);
 
 /* Counters of the reference's self-checks that print and continue
  * (Decomposition.h:158-170 and :273-277), accumulated since the last reset. */

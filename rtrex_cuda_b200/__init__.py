@@ -104,7 +104,12 @@ def lib():
     L.rtr_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.rtr_get_tuning.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rtr_autotune.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rtr_set_count_mode.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    L.rtr_get_count_mode.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rtr_graph_create_rmat.argtypes = [ctypes.c_int, _i64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_uint64, ctypes.c_int, P(_vp)]
     L.rtr_set_clean_split.argtypes = [_vp, _i64, ctypes.c_double]
+    L.rtr_set_clean_checks.argtypes = [_vp, _i64, _i64]
     L.rtr_get_clean_split.argtypes = [_vp, P(_i64), P(ctypes.c_double)]
     L.rtr_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, _i64, ctypes.c_int, P(_vp)]
     L.rtr_server_add_graph.argtypes = [_vp, _vp, _vp, _i64, _i64, ctypes.c_int, P(_i64)]
@@ -199,6 +204,15 @@ class Graph:
         h = _vp()
         _check(lib().rtr_graph_create_from_escape_file(path.encode(), int(device),
                                                         RTR_FLAG_SIMPLIFY if simplify else 0, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_rmat(cls, scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+                  seed: int = 3, device: int = 0) -> "Graph":
+        """R-MAT graph generated on the device (graphgen.rmat_hashed is the same graph in numpy)."""
+        h = _vp()
+        _check(lib().rtr_graph_create_rmat(int(scale), int(edge_factor), float(a), float(b), float(c),
+                                           int(seed) & ((1 << 64) - 1), int(device), ctypes.byref(h)))
         return cls(h.value)
 
     @classmethod
@@ -326,11 +340,28 @@ class Graph:
         """Counting work split (results are identical for every setting)."""
         _check(lib().rtr_set_tuning(self._h, int(gallop_ratio), int(heavy_degree), int(heavy_edge)))
 
+    def set_count_mode(self, mode: int, hub_degree: int = 4096):
+        """Counting layout: 0 keep triangle lists when they fit (default), 1 always,
+        2 never (rows layout: folds straight from the CSR rows; same bits, but the
+        clean needs the lists).  Vertices of at least hub_degree neighbours are
+        folded by a thread block in the rows layout."""
+        _check(lib().rtr_set_count_mode(self._h, int(mode), int(hub_degree)))
+
+    def count_mode(self):
+        """(mode, hub_degree, lists kept by the last count)."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().rtr_get_count_mode(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return int(a.value), int(b.value), bool(c.value)
+
     def set_clean_split(self, min_seeds: int, max_mean_list: float = 8.0):
         """Clean units with at least `min_seeds` seeds and triangle lists of at
         most `max_mean_list` entries on average replay in parallel rounds (one
         thread block each), the others one warp per unit (same bits)."""
         _check(lib().rtr_set_clean_split(self._h, int(min_seeds), float(max_mean_list)))
+
+    def set_clean_checks(self, first_wait_rounds: int = 0, stack_entries: int = -1):
+        """Lower the clean's device-side check bounds (to test their error reports)."""
+        _check(lib().rtr_set_clean_checks(self._h, int(first_wait_rounds), int(stack_entries)))
 
     def clean_split(self):
         v, x = _i64(), ctypes.c_double()

@@ -116,6 +116,10 @@ int copy_i32_as_i64(rtr_graph* g, const int32_t* d, int64_t k, int64_t* h)
 
 }  // namespace
 
+namespace rtr {
+int make_graph_handle(int64_t n, int device, rtr_graph** out) { return make_graph(n, device, out); }
+}  // namespace rtr
+
 extern "C" {
 
 const char* rtr_version(void) { return "rtrex-b200 0.1 (sm_100a)"; }
@@ -361,6 +365,29 @@ int rtr_set_tuning(rtr_graph* g, int gallop_ratio, int heavy_degree, int heavy_e
     return RTR_OK;
 }
 
+int rtr_set_count_mode(rtr_graph* g, int mode, int hub_degree)
+{
+    if (!g || mode < 0 || mode > 2 || hub_degree < 1) {
+        set_error("rtr_set_count_mode: null graph, mode outside 0..2 or hub_degree below 1");
+        return RTR_ERR_ARG;
+    }
+    g->count_mode = mode;
+    g->count_hub = hub_degree;
+    return RTR_OK;
+}
+
+int rtr_get_count_mode(const rtr_graph* g, int* mode, int* hub_degree, int* lists_kept)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    if (mode) *mode = g->count_mode;
+    if (hub_degree) *hub_degree = g->count_hub;
+    if (lists_kept) *lists_kept = g->lists ? 1 : 0;
+    return RTR_OK;
+}
+
 int rtr_set_clean_split(rtr_graph* g, int64_t min_seeds, double max_mean_list)
 {
     if (!g || min_seeds < 1 || !(max_mean_list >= 0)) {
@@ -369,6 +396,17 @@ int rtr_set_clean_split(rtr_graph* g, int64_t min_seeds, double max_mean_list)
     }
     g->clean_round_min = min_seeds;
     g->clean_round_list = max_mean_list;
+    return RTR_OK;
+}
+
+int rtr_set_clean_checks(rtr_graph* g, int64_t first_wait_rounds, int64_t stack_entries)
+{
+    if (!g || first_wait_rounds < 0 || stack_entries < -1) {
+        set_error("rtr_set_clean_checks: null graph, negative wait rounds or stack entries below -1");
+        return RTR_ERR_ARG;
+    }
+    g->clean_wait_first = first_wait_rounds;
+    g->clean_stack_limit = stack_entries;
     return RTR_OK;
 }
 

@@ -208,12 +208,12 @@ __global__ void k_unit_finish(UnitDesc* __restrict__ units, const int64_t* __res
                               const int64_t* __restrict__ capoff, int64_t nu, int64_t ns,
                               const uint32_t* __restrict__ ecount, const unsigned long long* __restrict__ tsum,
                               int64_t round_min, double round_max_list, uint64_t* __restrict__ order_keys,
-                              unsigned* __restrict__ nbig)
+                              unsigned* __restrict__ nbig, int64_t stack_limit)
 {
     for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < nu; u += (int64_t)gridDim.x * blockDim.x) {
         units[u].seed_end = (u + 1 < nu) ? units[u + 1].seed_begin : ns;
         units[u].stack_base = capoff[u];
-        units[u].stack_cap = cap[u];
+        units[u].stack_cap = (stack_limit >= 0 && cap[u] > stack_limit) ? stack_limit : cap[u];
         const uint64_t work = (uint64_t)(units[u].seed_end - units[u].seed_begin);
         const int64_t r = units[u].root;
         const bool rounds = (int64_t)work >= round_min && (double)tsum[r] <= round_max_list * (double)ecount[r];
@@ -244,6 +244,7 @@ struct CleanArgs {
     double* pv;
     double inv_n;
     const StackEntry* seeds;
+    long wait_first;  // try_wait rounds of a window's first wait (kWaitLimit unless lowered to test the report)
 };
 
 constexpr int kCleanBlock = 128;
@@ -603,9 +604,9 @@ __global__ void __launch_bounds__(kCleanBlock)
                         __syncwarp();
                         if (bytes) bulk_to_smem(&sm.went[lane][0], a.tl + wseed.t0, bytes, &sm.bar);
                         long it = 0;
-                        while (!mbar_done(&sm.bar, bar_phase) && ++it < kWaitLimit) {
+                        while (!mbar_done(&sm.bar, bar_phase) && ++it < a.wait_first) {
                         }
-                        if (it >= kWaitLimit) {  // report, give the copies one more bounded wait, stop
+                        if (it >= a.wait_first) {  // report, give the copies one more bounded wait, stop
                             if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_WAIT);
                             for (long j = 0; j < kWaitLimit && !mbar_done(&sm.bar, bar_phase); ++j) {
                             }
@@ -646,6 +647,12 @@ int initial_clean(rtr_graph* g, double eps)
     if (g->stage < 2) {
         set_error("clean called before count");
         return RTR_ERR_STATE;
+    }
+    if (!g->lists) {
+        set_error("the graph was counted in the rows layout (its triangle lists did not fit in device memory, "
+                  "or the count mode forbade them); the clean replays need the lists -- count again with "
+                  "rtr_set_count_mode(g, 1, ...) on a device with room for them");
+        return RTR_ERR_LIMIT;
     }
     cudaStream_t s = g->stream;
     const int64_t n = g->n, m = g->m, m2 = g->m2;
@@ -732,7 +739,7 @@ int initial_clean(rtr_graph* g, double eps)
         exclusive_scan_i64(cap, capoff, nu, d_cap_total, ctmp, s);
         k_unit_finish<<<grid_for(nu, kBlock), kBlock, 0, s>>>(units, cap, capoff, nu, ns, ecount, tsum,
                                                               g->clean_round_min, g->clean_round_list, okeys,
-                                                              next_unit + 1);
+                                                              next_unit + 1, g->clean_stack_limit);
         uint64_t* order = radix_sort_u64(okeys, oalt, nu, 64, otmp, s);
         g->launches += 5 + 24;
         int64_t cap_total = 0;
@@ -760,7 +767,8 @@ int initial_clean(rtr_graph* g, double eps)
             RTR_CUDA_TRY(cudaEventRecord(joined, g->side));
         }
         if ((int64_t)nbig < (int64_t)nu) {
-            CleanArgs ca{g->tl, rec, g->pv, 1 / (double)n, seeds};
+            CleanArgs ca{g->tl, rec, g->pv, 1 / (double)n, seeds,
+                         g->clean_wait_first > 0 ? (long)g->clean_wait_first : kWaitLimit};
             // one warp per unit, persistent over the unit list (largest units first)
             const int64_t nsmall = (int64_t)nu - (int64_t)nbig;
             int blocks = (int)std::min<int64_t>((nsmall + kCleanWarps - 1) / kCleanWarps,
@@ -793,7 +801,12 @@ int initial_clean(rtr_graph* g, double eps)
     unsigned long long h[3];
     RTR_CUDA_TRY(cudaMemcpy(h, g->ctr, sizeof h, cudaMemcpyDeviceToHost));
     if (h[1] != 0) {
-        set_error("device error word 0x%llx during the clean", h[1]);
+        set_error("device error word 0x%llx during the clean:%s%s%s%s%s", h[1],
+                  (h[1] & DEV_ERR_STACK_OVERFLOW) ? " a unit's cascade stack overflowed its region;" : "",
+                  (h[1] & DEV_ERR_BAD_STATUS) ? " an edge record held an impossible status;" : "",
+                  (h[1] & DEV_ERR_SCRATCH) ? " a support count exceeded its field;" : "",
+                  (h[1] & DEV_ERR_SORT) ? " a sort key left its range;" : "",
+                  (h[1] & DEV_ERR_WAIT) ? " a bounded wait on an asynchronous copy ran out;" : "");
         return RTR_ERR_DEVICE;
     }
     g->diag_residual = (long long)h[2];

@@ -26,6 +26,7 @@
 // which a vertex is folded by a warp; g->tune_edge: the degree sum from which an
 // edge is intersected by a warp) change how work is spread, never a result; the
 // autotuner (rtr_autotune) times candidates on the graph itself.
+#include "intersect.cuh"
 #include "primitives.cuh"
 #include "rtr_graph.cuh"
 
@@ -34,118 +35,6 @@ namespace rtr {
 namespace {
 
 constexpr int kBlock = 256;
-
-// Visit common neighbours of rows [a0,a1) and [b0,b1) in ascending order:
-// f(z, slot_in_a, slot_in_b).  Skewed pairs gallop the short row into the long.
-template <typename F>
-__device__ __forceinline__ void intersect_rows(const int32_t* __restrict__ nb, int64_t a0, int64_t a1, int64_t b0,
-                                               int64_t b1, int gallop, F&& f)
-{
-    const int64_t la = a1 - a0, lb = b1 - b0;
-    if (la == 0 || lb == 0) return;
-    if (la * gallop < lb || lb * gallop < la) {
-        const bool a_short = la <= lb;
-        const int64_t s0 = a_short ? a0 : b0, s1 = a_short ? a1 : b1;
-        int64_t lo = a_short ? b0 : a0;
-        const int64_t l1 = a_short ? b1 : a1;
-        for (int64_t p = s0; p < s1 && lo < l1; ++p) {
-            const int32_t x = nb[p];
-            int64_t hi = l1;
-            while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (nb[mid] < x) lo = mid + 1;
-                else hi = mid;
-            }
-            if (lo < l1 && nb[lo] == x) {
-                if (a_short) f(x, p, lo);
-                else f(x, lo, p);
-                ++lo;
-            }
-        }
-        return;
-    }
-    int64_t i = a0, j = b0;
-    int32_t x = nb[i], y = nb[j];
-    while (true) {
-        if (x < y) {
-            if (++i >= a1) break;
-            x = nb[i];
-        } else if (x > y) {
-            if (++j >= b1) break;
-            y = nb[j];
-        } else {
-            f(x, i, j);
-            if (++i >= a1 || ++j >= b1) break;
-            x = nb[i];
-            y = nb[j];
-        }
-    }
-}
-
-__device__ __forceinline__ int64_t lower_bound_row(const int32_t* __restrict__ nb, int64_t lo, int64_t hi, int32_t x)
-{
-    while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (nb[mid] < x) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Lane `lane`'s share of the common neighbours of rows A=[a0,a1) and B=[b0,b1),
-// visited in ascending order: f(z, slot_in_a, slot_in_b).  The shorter row is
-// cut into 32 contiguous pieces and the lane takes piece `lane` together with
-// the part of the longer row between its piece's first value and the next
-// piece's first value, so lane l's common neighbours all precede lane l+1's.
-// Within its part a lane merges, or -- when the rows' lengths differ by more
-// than `gallop` -- binary-searches each of its elements.
-template <typename F>
-__device__ __forceinline__ void warp_intersect_part(const int32_t* __restrict__ nb, int64_t a0, int64_t a1, int64_t b0,
-                                                    int64_t b1, int gallop, int lane, F&& f)
-{
-    const int64_t la = a1 - a0, lb = b1 - b0;
-    if (la == 0 || lb == 0) return;
-    const bool a_short = la <= lb;
-    const int64_t s0 = a_short ? a0 : b0, s1 = a_short ? a1 : b1;
-    const int64_t l0 = a_short ? b0 : a0, l1 = a_short ? b1 : a1;
-    const int64_t ls = s1 - s0, ll = l1 - l0;
-    const int64_t piece = (ls + 31) / 32;
-    const int64_t p0 = s0 + (int64_t)lane * piece;
-    const int64_t p1 = p0 + piece < s1 ? p0 + piece : s1;
-    if (p0 >= p1) return;
-    int64_t lo = lower_bound_row(nb, l0, l1, nb[p0]);
-    const int64_t hi = p1 < s1 ? lower_bound_row(nb, lo, l1, nb[p1]) : l1;
-    if (ls * gallop < ll) {
-        for (int64_t p = p0; p < p1 && lo < hi; ++p) {
-            const int32_t x = nb[p];
-            lo = lower_bound_row(nb, lo, hi, x);
-            if (lo < hi && nb[lo] == x) {
-                if (a_short) f(x, p, lo);
-                else f(x, lo, p);
-                ++lo;
-            }
-        }
-        return;
-    }
-    int64_t i = p0, j = lo;
-    if (j >= hi) return;
-    int32_t x = nb[i], y = nb[j];
-    while (true) {
-        if (x < y) {
-            if (++i >= p1) break;
-            x = nb[i];
-        } else if (x > y) {
-            if (++j >= hi) break;
-            y = nb[j];
-        } else {
-            if (a_short) f(x, i, j);
-            else f(x, j, i);
-            if (++i >= p1 || ++j >= hi) break;
-            x = nb[i];
-            y = nb[j];
-        }
-    }
-}
 
 __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long* dst)
 {
@@ -467,6 +356,37 @@ int count_triangles(rtr_graph* g)
     int64_t tl_len = 0;
     RTR_CUDA_TRY(cudaMemcpyAsync(&tl_len, g->tl_off + m2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    bool keep_lists = g->count_mode != 2;
+    if (g->count_mode == 0 && (tl_len > g->tl_len || !g->tl)) {
+        // keep the lists only when they fit beside what the clean will need (records, stacks)
+        size_t free_b = 0, total_b = 0;
+        RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        const double need = (double)sizeof(TriEntry) * (double)(tl_len + 1) + 64.0 * (double)(m + 1) +
+                            (double)(1ll << 30);
+        keep_lists = need <= (double)free_b;
+    }
+    if (!keep_lists) {
+        // rows layout: perVertex and heavy-edge perEdge straight from the CSR rows
+        g->lists = false;
+        g->tl_len = 0;
+        ktime_begin(g, KT_TRI_FILL);
+        ktime_end(g, KT_TRI_FILL);
+        ktime_begin(g, KT_VERTEX_FOLD);
+        const int rc = count_rows(g, sc);
+        ktime_end(g, KT_VERTEX_FOLD);
+        if (rc) return rc;
+        RTR_CUDA_TRY(cudaGetLastError());
+        cudaEventRecord(e1, s);
+        RTR_CUDA_TRY(cudaEventSynchronize(e1));
+        cudaEventElapsedTime(&g->ms_count, e0, e1);
+        ktime_read(g, KT_EDGE_FOLD);
+        ktime_read(g, KT_TRI_FILL);
+        ktime_read(g, KT_VERTEX_FOLD);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        g->stage = 2;
+        return RTR_OK;
+    }
     if (tl_len > g->tl_len || !g->tl) {
         // grow-only buffer owned by the graph
         g->tl = (TriEntry*)dev_alloc(g, sizeof(TriEntry) * (tl_len + 1));
@@ -476,6 +396,7 @@ int count_triangles(rtr_graph* g)
         }
     }
     g->tl_len = tl_len;
+    g->lists = true;
     ktime_begin(g, KT_TRI_FILL);
     k_tri_fill<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->partner, g->fwd, g->frank, m,
                                      g->tl_off, g->tl, g->tune_gallop, g->tune_edge);

@@ -1,0 +1,319 @@
+// List-free weighted triangle counting ("rows" layout): perVertex and the
+// perEdge of heavy edges folded straight from the CSR rows, with no
+// per-triangle storage, for graphs whose triangle lists do not fit in HBM
+// (R-MAT scale 22 already has 2.1 G triangles, i.e. ~200 GB of lists; scale 24
+// 10.3 G).  commonNbr itself keeps no lists either
+// (RTRex_Sequential/Escape/Decomposition.h:70-115): it re-intersects rows.
+//
+// What runs before this (count.cu): k_edge_fold folds perEdge for every light
+// edge (deg u + deg v below the heavy-edge threshold) and k_edge_count_heavy
+// counts the heavy ones, so support, the triangle total and light perEdge are
+// known.  This file adds, bit-exact to commonNbr's discovery order:
+//   perVertex[x] = left fold over y in N(x) ascending, then over
+//                  z in N(x) & N(y), z > y ascending, of 1/double(dx*dy*dz)
+//   perEdge[(x,y)] for heavy edges, x < y = left fold over z in N(x) & N(y)
+//                  ascending, computed by x's pass from the same intersection.
+// For y > x owning a heavy edge the pass intersects the full rows (perEdge
+// needs every z; the z > y suffix continues perVertex[x]); otherwise it
+// intersects N(x) beyond y with N(y).
+//
+// Three kernels by the degree of x:
+//   k_rows_light   a thread per vertex of degree < light (merge / gallop)
+//   k_rows_medium  a warp per vertex of degree in [light, hub): for each y in
+//                  turn the warp walks the shorter row 32 elements at a time,
+//                  every lane binary-searching its element in the longer one,
+//                  and folds the hits in lane order (ascending z)
+//   k_rows_hub     a thread block per vertex of degree >= hub, hubs in
+//                  descending degree: the block's 8 warps take 8 consecutive y
+//                  at once, searching x's row through a shared-memory sample of
+//                  it (every stride-th element) and a one-window global search;
+//                  each warp writes its y's z > y weights, in order, to its own
+//                  buffer, and warp 0 then folds the 8 buffers in y order --
+//                  only the perVertex chain itself is sequential.
+// The hub kernel runs on the graph's second stream, concurrently with the
+// other two (it holds the longest dependent chain: ~10^8 adds for the largest
+// R-MAT scale-24 hub).
+#include "intersect.cuh"
+#include "primitives.cuh"
+#include "rtr_graph.cuh"
+
+namespace rtr {
+
+namespace {
+
+constexpr int kLightBlock = 256;
+constexpr int kMediumBlock = 128;
+constexpr int kHubWarps = 8;
+constexpr int kHubBlock = 32 * kHubWarps;
+constexpr int kHubIndexMax = 11264;  // sample entries of a hub row in shared memory (44 KB, static limit 48 KB)
+
+struct RowsArgs {
+    const int64_t* off;
+    const int32_t* nb;
+    const int32_t* deg;
+    int64_t n;
+    double* pe;
+    double* pv;
+    int gallop;
+    int heavy_edge;  // deg x + deg y from which perEdge is folded here (k_edge_fold left it)
+    int light;       // vertices below this degree: a thread
+    int hub;         // vertices from this degree: a thread block
+};
+
+__device__ __forceinline__ bool owns_heavy(const RowsArgs& a, int32_t x, int32_t y, int dx, int dy)
+{
+    return x < y && dx + dy >= a.heavy_edge;
+}
+
+__global__ void __launch_bounds__(kLightBlock) k_rows_light(RowsArgs a)
+{
+    for (int64_t xi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; xi < a.n;
+         xi += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t x = (int32_t)xi;
+        const int dx = a.deg[x];
+        if (dx >= a.light) continue;
+        const int64_t a0 = a.off[x], a1 = a.off[x + 1];
+        double pvacc = 0.0;
+        for (int64_t i = a0; i < a1; ++i) {
+            const int32_t y = a.nb[i];
+            const int dy = a.deg[y];
+            const int64_t dxy = (int64_t)dx * (int64_t)dy;
+            const int64_t b0 = a.off[y], b1 = a.off[y + 1];
+            if (owns_heavy(a, x, y, dx, dy)) {
+                double peacc = 0.0;
+                intersect_rows(a.nb, a0, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) {
+                    const double w = 1.0 / (double)(dxy * (int64_t)a.deg[z]);
+                    peacc += w;
+                    if (z > y) pvacc += w;
+                });
+                a.pe[i] = peacc;
+            } else {
+                intersect_rows(a.nb, i + 1, a1, b0, b1, a.gallop,
+                               [&](int32_t z, int64_t, int64_t) { pvacc += 1.0 / (double)(dxy * (int64_t)a.deg[z]); });
+            }
+        }
+        a.pv[x] = pvacc;
+    }
+}
+
+__global__ void __launch_bounds__(kMediumBlock) k_rows_medium(RowsArgs a)
+{
+    __shared__ double s_w[kMediumBlock / 32][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t nwarps = (int64_t)gridDim.x * (kMediumBlock / 32);
+    auto search = [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(a.nb, lo, hi, v); };
+    for (int64_t xi = (int64_t)blockIdx.x * (kMediumBlock / 32) + wib; xi < a.n; xi += nwarps) {
+        const int32_t x = (int32_t)xi;
+        const int dx = a.deg[x];
+        if (dx < a.light || dx >= a.hub) continue;  // uniform across the warp
+        const int64_t a0 = a.off[x], a1 = a.off[x + 1];
+        double pvacc = 0.0;
+        for (int64_t i = a0; i < a1; ++i) {
+            const int32_t y = a.nb[i];
+            const int dy = a.deg[y];
+            const int64_t dxy = (int64_t)dx * (int64_t)dy;
+            const bool owner = owns_heavy(a, x, y, dx, dy);
+            const int64_t A0 = owner ? a0 : i + 1, A1 = a1;
+            int64_t B0 = a.off[y];
+            const int64_t B1 = a.off[y + 1];
+            if (!owner && B1 - B0 <= A1 - A0) B0 = lower_bound_row(a.nb, B0, B1, y + 1);  // A holds only z > y
+            double peacc = 0.0;
+            auto chunk = [&](bool hit, int32_t z) {
+                const double w = hit ? 1.0 / (double)(dxy * (int64_t)a.deg[z]) : 0.0;
+                const int below = owner ? __popc(__ballot_sync(0xffffffffu, hit && z < y)) : 0;
+                fold_hits(hit, w, s_w[wib], lane, owner ? &peacc : nullptr, &pvacc, below);
+            };
+            if (A1 - A0 <= B1 - B0) warp_chunks(a.nb, A0, A1, B0, B1, lane, search, chunk);
+            else warp_chunks(a.nb, B0, B1, A0, A1, lane, search, chunk);
+            if (owner && lane == 0) a.pe[i] = peacc;
+        }
+        if (lane == 0) a.pv[x] = pvacc;
+    }
+}
+
+// Hubs: hubs[] in descending degree; buf holds kHubWarps regions of cap
+// doubles per block (cap >= the largest hub degree, which bounds the z > y
+// hits of one y).
+__global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_t* __restrict__ hubs, int64_t nhub,
+                                                         double* __restrict__ buf, int64_t cap)
+{
+    __shared__ int32_t s_idx[kHubIndexMax];
+    __shared__ double s_w[kHubWarps][32];
+    __shared__ int64_t s_len[kHubWarps];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* region = buf + ((int64_t)blockIdx.x * kHubWarps + wib) * cap;
+    for (int64_t h = blockIdx.x; h < nhub; h += gridDim.x) {
+        const int32_t x = hubs[h];
+        const int dx = a.deg[x];
+        const int64_t a0 = a.off[x], a1 = a.off[x + 1], d = a1 - a0;
+        int64_t stride = (d + kHubIndexMax - 1) / kHubIndexMax;
+        if (stride < 32) stride = 32;
+        const int K = (int)((d + stride - 1) / stride);
+        for (int k = threadIdx.x; k < K; k += kHubBlock) s_idx[k] = a.nb[a0 + (int64_t)k * stride];
+        __syncthreads();
+        // lower bound of v in x's whole row: the sample narrows it to one window
+        auto search_x = [&](int64_t, int64_t, int32_t v) -> int64_t {
+            int lo = 0, hi = K;  // first sample above v
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (s_idx[mid] <= v) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo == 0) return a0;
+            const int64_t w0 = a0 + (int64_t)(lo - 1) * stride;
+            const int64_t w1 = w0 + stride < a1 ? w0 + stride : a1;
+            return lower_bound_row(a.nb, w0, w1, v);
+        };
+        auto search_g = [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(a.nb, lo, hi, v); };
+        double pvacc = 0.0;  // meaningful in warp 0
+        for (int64_t base = a0; base < a1; base += kHubWarps) {
+            const int64_t i = base + wib;
+            int64_t len = 0;
+            if (i < a1) {  // uniform across the warp
+                const int32_t y = a.nb[i];
+                const int dy = a.deg[y];
+                const int64_t dxy = (int64_t)dx * (int64_t)dy;
+                const bool owner = owns_heavy(a, x, y, dx, dy);
+                const int64_t A0 = owner ? a0 : i + 1, A1 = a1;
+                int64_t B0 = a.off[y];
+                const int64_t B1 = a.off[y + 1];
+                double peacc = 0.0;
+                auto chunk = [&](bool hit, int32_t z) {
+                    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+                    const int cnt = __popc(mask);
+                    if (cnt == 0) return;
+                    const double w = hit ? 1.0 / (double)(dxy * (int64_t)a.deg[z]) : 0.0;
+                    const int below = owner ? __popc(__ballot_sync(0xffffffffu, hit && z < y)) : 0;
+                    const int rank = __popc(mask & ((1u << lane) - 1u));
+                    if (owner) fold_hits(hit, w, s_w[wib], lane, &peacc, nullptr, 0);
+                    if (hit && rank >= below) region[len + rank - below] = w;
+                    len += cnt - below;
+                };
+                if (B1 - B0 <= A1 - A0) {
+                    if (!owner) B0 = lower_bound_row(a.nb, B0, B1, y + 1);  // A holds only z > y
+                    warp_chunks(a.nb, B0, B1, A0, A1, lane, search_x, chunk);
+                } else {
+                    warp_chunks(a.nb, A0, A1, B0, B1, lane, search_g, chunk);
+                }
+                if (owner && lane == 0) a.pe[i] = peacc;
+            }
+            if (lane == 0) s_len[wib] = len;
+            __syncthreads();
+            if (wib == 0) {
+                for (int w = 0; w < kHubWarps; ++w) {
+                    const int64_t L = s_len[w];
+                    const double* r = buf + ((int64_t)blockIdx.x * kHubWarps + w) * cap;
+                    double v = lane < L ? r[lane] : 0.0;
+                    for (int64_t k0 = 0; k0 < L; k0 += 32) {
+                        const double vn = k0 + 32 + lane < L ? r[k0 + 32 + lane] : 0.0;  // next 32, ahead of the chain
+                        const int c = L - k0 < 32 ? (int)(L - k0) : 32;
+                        double t[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) t[j] = __shfl_sync(0xffffffffu, v, j);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (j < c) pvacc += t[j];
+                        v = vn;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) a.pv[x] = pvacc;
+        __syncthreads();
+    }
+}
+
+__global__ void k_hub_keys(const int32_t* __restrict__ deg, int64_t n, int hub, uint64_t* __restrict__ keys,
+                           unsigned* __restrict__ nh)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        if (deg[v] >= hub)
+            keys[atomicAdd(nh, 1u)] = ((uint64_t)(0x7fffffff - deg[v]) << 32) | (uint64_t)v;
+}
+
+__global__ void k_hub_ids(const uint64_t* __restrict__ keys, int64_t nh, int32_t* __restrict__ ids)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nh; i += (int64_t)gridDim.x * blockDim.x)
+        ids[i] = (int32_t)(keys[i] & 0xffffffffu);
+}
+
+}  // namespace
+
+// perVertex (all vertices) and heavy-edge perEdge from the rows; the caller has
+// run the edge fold and heavy-edge count.  Synchronises the graph's stream.
+int count_rows(rtr_graph* g, Scratch& sc)
+{
+    cudaStream_t s = g->stream;
+    const int64_t n = g->n;
+    RowsArgs a{g->offsets, g->nbors, g->deg, n, g->pe, g->pv, g->tune_gallop, g->tune_edge, g->tune_heavy,
+               g->count_hub};
+    if (a.hub < a.light) a.hub = a.light;
+    uint64_t* keys = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
+    uint64_t* alt = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
+    unsigned* d_nh = (unsigned*)sc.get(sizeof(unsigned) * 2);
+    if (!keys || !alt || !d_nh) {
+        set_error("device allocation failed (hub list)");
+        return RTR_ERR_CUDA;
+    }
+    RTR_CUDA_TRY(cudaMemsetAsync(d_nh, 0, sizeof(unsigned), s));
+    k_hub_keys<<<grid_for(n, 256), 256, 0, s>>>(g->deg, n, a.hub, keys, d_nh);
+    unsigned nh = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&nh, d_nh, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    g->launches += 1;
+    int32_t* hubs = nullptr;
+    double* hbuf = nullptr;
+    int64_t cap = 0;
+    int hub_grid = 0;
+    if (nh > 0) {
+        void* rtmp = sc.get(radix_temp_bytes(nh));
+        hubs = (int32_t*)sc.get(sizeof(int32_t) * (nh + 1));
+        if (!rtmp || !hubs) {
+            set_error("device allocation failed (hub list)");
+            return RTR_ERR_CUDA;
+        }
+        uint64_t* sorted = radix_sort_u64(keys, alt, nh, 64, rtmp, s);
+        uint64_t first = 0;
+        RTR_CUDA_TRY(cudaMemcpyAsync(&first, sorted, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        k_hub_ids<<<grid_for(nh, 256), 256, 0, s>>>(sorted, nh, hubs);
+        RTR_CUDA_TRY(cudaStreamSynchronize(s));
+        g->launches += 1 + 3 * 8;
+        cap = (int64_t)(0x7fffffff - (int64_t)(first >> 32));  // the largest hub degree
+        int dev_sms = 148;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device);
+        hub_grid = (int)((int64_t)nh < dev_sms ? (int64_t)nh : dev_sms);
+        hbuf = (double*)sc.get(sizeof(double) * (size_t)hub_grid * kHubWarps * (size_t)(cap + 32));
+        if (!hbuf) {
+            set_error("device allocation failed (hub fold buffers, %lld hubs of degree up to %lld)", (long long)nh,
+                      (long long)cap);
+            return RTR_ERR_CUDA;
+        }
+        cap += 32;
+    }
+    cudaEvent_t ready = nullptr, joined = nullptr;
+    if (hub_grid > 0) {
+        if (!g->side) RTR_CUDA_TRY(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking));
+        RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
+        RTR_CUDA_TRY(cudaEventRecord(ready, s));
+        RTR_CUDA_TRY(cudaStreamWaitEvent(g->side, ready, 0));
+        k_rows_hub<<<hub_grid, kHubBlock, 0, g->side>>>(a, hubs, nh, hbuf, cap);
+        RTR_CUDA_TRY(cudaEventRecord(joined, g->side));
+        g->launches += 1;
+    }
+    k_rows_light<<<grid_for(n, kLightBlock), kLightBlock, 0, s>>>(a);
+    k_rows_medium<<<grid_for(1ll << 40, kMediumBlock, 16), kMediumBlock, 0, s>>>(a);
+    g->launches += 2;
+    cudaError_t e = cudaGetLastError();
+    if (joined) {
+        cudaStreamWaitEvent(s, joined, 0);
+        cudaStreamSynchronize(s);  // scratch (hub list, buffers) is freed on return
+        cudaEventDestroy(ready);
+        cudaEventDestroy(joined);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "rows-layout counting launch", __FILE__, __LINE__);
+    return RTR_OK;
+}
+
+}  // namespace rtr

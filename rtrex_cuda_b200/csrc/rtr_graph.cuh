@@ -77,11 +77,21 @@ struct rtr_graph {
     int tune_gallop = 16;
     int tune_heavy = 32;
     int tune_edge = 1024;  // deg u + deg v from which an edge is intersected by a warp
+    // counting layout: 0 keep triangle lists when they fit in free device memory,
+    // 1 always keep them, 2 never (rows layout: folds straight from the CSR);
+    // count_hub: degree from which the rows layout gives a vertex a thread block
+    int count_mode = 0;
+    int count_hub = 4096;
+    bool lists = false;  // the last count kept the triangle lists (the clean needs them)
     // clean units with at least this many seeds and triangle lists of at most
     // this mean length replay in parallel rounds (one thread block each); the
     // others one warp per unit
     int64_t clean_round_min = 2048;
     double clean_round_list = 8.0;
+    // bounds of the clean's device-side checks, lowered only to test their reports:
+    // try_wait rounds of a window's first wait (0: the full limit), unit stack entries (-1: as sized)
+    int64_t clean_wait_first = 0;
+    int64_t clean_stack_limit = -1;
     cudaStream_t side = nullptr;  // second stream of the graph (created on first use)
 
     // stage timings from CUDA events (ms)
@@ -133,6 +143,8 @@ struct Scratch {
 int build_csr(rtr_graph* g, const int64_t* d_u, const int64_t* d_v, int64_t m, bool simplify);
 int build_csr_from_host_csr(rtr_graph* g, const int64_t* h_offsets, const int64_t* h_nbors);
 int count_triangles(rtr_graph* g);
+int count_rows(rtr_graph* g, Scratch& sc);  // list-free perVertex / heavy perEdge (count_rows.cu)
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 int initial_clean(rtr_graph* g, double eps);
 int extract_clusters(rtr_graph* g);
 int connected_components(rtr_graph* g);

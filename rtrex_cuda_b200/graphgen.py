@@ -25,7 +25,7 @@ import os
 import numpy as np
 
 __all__ = [
-    "simplify", "gnp_cliques", "chung_lu", "rmat", "sbm", "small_test",
+    "simplify", "gnp_cliques", "chung_lu", "rmat", "rmat_hashed", "rmat_hashed_pairs", "sbm", "small_test",
     "write_escape", "read_escape", "parse_escape", "config_graph",
 ]
 
@@ -150,6 +150,59 @@ def rmat(scale=24, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3, chunk=1 << 24
         done += k
     key = np.unique(np.concatenate(keys))
     return n, key // n, key % n
+
+
+_MIX_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """splitmix64 output function (Steele, Lea, Flood 2014) on uint64 arrays."""
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def _threshold32(p: float) -> int:
+    if not p > 0.0:
+        return 0
+    if p >= 1.0:
+        return 1 << 32
+    return int(np.floor(p * 4294967296.0))
+
+
+def rmat_hashed_pairs(scale=24, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3, chunk=1 << 22):
+    """The raw generated pairs of rtr_graph_create_rmat (before symmetrising):
+    pair k's bit at level l comes from mix64(seed * golden ^ (k << 6 | l)); the
+    high 32 bits decide the source half, the low 32 bits the destination half."""
+    M = edge_factor << scale
+    t_ab, t_a, t_c = (np.uint64(_threshold32(p)) for p in (a + b, a / (a + b), c / (1.0 - a - b)))
+    smix = np.uint64((int(seed) * 0x9E3779B97F4A7C15) & ((1 << 64) - 1))
+    src = np.empty(M, np.int64)
+    dst = np.empty(M, np.int64)
+    with np.errstate(over="ignore"):
+        for k0 in range(0, M, chunk):
+            k = np.arange(k0, min(M, k0 + chunk), dtype=np.uint64)
+            s = np.zeros(k.size, np.uint64)
+            t = np.zeros(k.size, np.uint64)
+            for lvl in range(scale):
+                h = _mix64(smix ^ ((k << np.uint64(6)) | np.uint64(lvl)))
+                hi = h >> np.uint64(32)
+                lo = h & np.uint64(0xFFFFFFFF)
+                ii = hi >= t_ab
+                jj = lo >= np.where(ii, t_c, t_a)
+                bit = np.uint64(scale - 1 - lvl)
+                s |= ii.astype(np.uint64) << bit
+                t |= jj.astype(np.uint64) << bit
+            src[k0:k0 + k.size] = s.astype(np.int64)
+            dst[k0:k0 + k.size] = t.astype(np.int64)
+    return 1 << scale, src, dst
+
+
+def rmat_hashed(scale=24, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=3):
+    """R-MAT graph of rtr_graph_create_rmat (device generator), simplified."""
+    n, src, dst = rmat_hashed_pairs(scale, edge_factor, a, b, c, seed)
+    u, v = simplify(n, src, dst)
+    return n, u, v
 
 
 def sbm(m_target: int, seed: int, mean_intra=12.0, mean_inter=2.0,

@@ -4,9 +4,11 @@ pre-reserves its HBM and hands out memory only from its own arena).
 
 The test owns all device buffers (torch tensors), calls the entry point through
 the C ABI, and checks its outputs bit for bit against the allocating path
-(rtr_count + rtr_get_weights) on consecutive calls with different graphs, so
-stale contents of the shared static scratch cannot leak between calls.  The
-file is named to be collected last.
+(rtr_count + rtr_get_weights) and against the reference's own commonNbr
+digests (tests/golden/golden.json) on consecutive calls with different graphs,
+so stale contents of the shared static scratch cannot leak between calls; a
+power-law graph sends its hubs through the warp-per-vertex kernel.  The file is
+named to be collected last.
 """
 import ctypes
 
@@ -53,7 +55,13 @@ def _call_noalloc(off, nb, n):
             int(d_tot.cpu().item()))
 
 
-@pytest.mark.parametrize("sequence", [("gnp_cliques", "sbm_3000_4002", "gnp_cliques")])
+def _golden_count(name):
+    """The reference's own commonNbr digests for the case (any threshold entry)."""
+    entry = helpers.golden()["cases"][name]
+    return next(iter(entry.values()))["count"]
+
+
+@pytest.mark.parametrize("sequence", [("gnp_cliques", "chung_lu", "sbm_3000_4002", "gnp_cliques")])
 def test_noalloc_matches_allocating_path_on_consecutive_calls(sequence):
     for name in sequence:
         n, u, v = helpers.case_graph(name)
@@ -63,6 +71,11 @@ def test_noalloc_matches_allocating_path_on_consecutive_calls(sequence):
         assert (helpers.bits(got_pe) == helpers.bits(pe)).all(), name
         assert (helpers.bits(got_pv) == helpers.bits(pv)).all(), name
         assert (got_sup == sup).all(), name
+        # and directly against the reference's digests (chung_lu's hubs go to the warp kernel)
+        gold = _golden_count(name)
+        assert got_total == gold["total"], name
+        assert helpers.sha(helpers.bits(got_pe).tobytes()) == gold["perEdge"], name
+        assert helpers.sha(helpers.bits(got_pv).tobytes()) == gold["perVertex"], name
 
 
 def test_noalloc_rejects_graphs_beyond_its_fixed_scratch():
@@ -72,3 +85,27 @@ def test_noalloc_rejects_graphs_beyond_its_fixed_scratch():
     rc = _entry()(p, p, (1 << 20) + 1, p, p, p, p, None)
     assert rc == 4
     assert b"exceeds the fixed scratch limit" in rtr.lib().rtr_last_error()
+
+
+def test_noalloc_rejects_null_buffers():
+    import torch
+    dummy = torch.zeros(4, dtype=torch.int64, device="cuda")
+    p = dummy.data_ptr()
+    for k in (1, 3, 5):  # d_nbors, d_perEdge, d_support
+        args = [p, p, 3, p, p, p, p, None]
+        args[k] = None
+        assert _entry()(*args) == 1
+        assert b"null buffer" in rtr.lib().rtr_last_error()
+
+
+def test_noalloc_reports_out_of_range_neighbours():
+    # a triangle 0-1-2 whose row 2 also names vertex 7 of a 3-vertex graph: the
+    # id is skipped (never dereferenced) and the total comes back as -1
+    off = np.array([0, 2, 4, 7], np.int64)
+    nb = np.array([1, 2, 0, 2, 0, 1, 7], np.int32)
+    _, _, _, total = _call_noalloc(off, nb, 3)
+    assert total == -1
+    off = np.array([0, 2, 4, 6], np.int64)
+    nb = np.array([1, 2, 0, 2, 0, 1], np.int32)
+    _, _, sup, total = _call_noalloc(off, nb, 3)
+    assert total == 1 and (sup == 1).all()  # the error word does not outlive its call
