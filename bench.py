@@ -61,13 +61,17 @@ def parse_args():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--skip-extras", action="store_true",
+                    help="leave out the R-MAT scale-24 count, batched and reference-GPU legs of the default run")
     ap.add_argument("--serve-requests", type=int, default=240)
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--serve-pool", type=int, default=32)
     ap.add_argument("--serve-max-edges", type=float, default=2e6)
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batch", "serve"],
+    ap.add_argument("--rmat-scale", type=int, default=24)
+    ap.add_argument("--count-mode", type=int, default=0, help="rtr_set_count_mode for --workload rmat_count")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batch", "serve", "rmat_count"],
                     help="batch: the 4,096-graph SBM batch, batched vs per-graph plain decompositions")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     return ap.parse_args()
@@ -291,6 +295,206 @@ def clean_bytes(n, off, nb, status, tri_removed):
     return int(4 * (deg[src[fwd]] + deg[nb[fwd]]).sum() + nb.size + 48 * tri_removed)
 
 
+def oriented_sum_chunked(off, nb, chunk=1 << 24):
+    """Sum over the degree-oriented edges u->v of d+(u) + d+(v), which equals the
+    sum over undirected edges of min(deg u, deg v); vertex chunks keep the host
+    memory bounded on graphs of hundreds of millions of edges."""
+    n = off.size - 1
+    deg = np.diff(off)
+    total = 0
+    a = 0
+    while a < n:
+        b = int(np.searchsorted(off, off[a] + chunk, side="right"))
+        b = max(b, a + 1)
+        b = min(b, n)
+        s0, s1 = int(off[a]), int(off[b])
+        src = np.repeat(np.arange(a, b, dtype=np.int64), deg[a:b])
+        dst = nb[s0:s1]
+        fwd = src < dst
+        total += int(np.minimum(deg[src[fwd]], deg[dst[fwd]]).sum())
+        a = b
+    return total
+
+
+def rmat24_leg(args, dev, flush_l2, peak, peak_kind, scale=24, steps=None, mode=0):
+    """R-MAT scale 24 (edge factor 16, a,b,c = .57,.19,.19, seed 3) counted on
+    the device: its triangle lists would need ~1 TB, so rtr_count folds
+    straight from the CSR rows.  Device-timed count steps (CUDA events; the
+    graph is resident and 4 GB of rows exceed L2), then end to end from pinned
+    host edges (H2D + CSR build + count + perVertex read back).  Other scales
+    (and a forced count mode) serve profiling."""
+    import torch
+    import rtrex_cuda_b200 as rtr
+    steps = max(1, min(args.steps, 3)) if steps is None else steps
+    g = rtr.Graph.from_rmat(scale, 16, seed=3, device=dev)
+    g.set_count_mode(mode)
+    gen_ms = g.stats()["ms_build"]
+    n, m = g.n, g.m
+    g.count()  # warm-up
+    ms, launches0 = [], g.stats()["launches"]
+    for k in range(steps):
+        flush_l2(k)
+        total = g.count()
+        ms.append(g.stats()["ms_count"])
+    launches = (g.stats()["launches"] - launches0) // steps
+    layout = "rows (no triangle lists)" if not g.count_mode()[2] else "triangle lists"
+    kms = g.kernel_ms()
+    off, nb = g.csr()
+    g.close()
+    osum = oriented_sum_chunked(off, nb)
+    b_count = 8 * (n + 1) + 4 * osum + 24 * m + 8 * n
+    t = float(np.mean(ms)) / 1e3
+    out = {"workload": f"rmat{scale}", "desc": f"R-MAT scale {scale}, edge factor 16, a,b,c,d = .57,.19,.19,.05, "
+                                                "seed 3, symmetrised, self-loops and repeats dropped (device generator)",
+           "n": n, "m": m, "triangles": total, "layout": layout, "steps": steps,
+           "ms_per_count": t * 1e3, "edges_per_s": m / t, "triangles_per_s": total / t,
+           "generation_and_csr_build_ms": gen_ms,
+           "kernel_ms": {"edge_fold_and_heavy_count": kms["k_edge_fold"], "rows_folds": kms["k_vertex_fold"]},
+           "gpu_launches_per_count": launches,
+           "roofline_count": {"bound": "hbm", "algorithmic_bytes": b_count, "oriented_sum": osum,
+                              "achieved": b_count / t / 1e9, "peak": peak, "unit": "GB/s",
+                              "frac": b_count / t / 1e9 / peak, "peak_kind": peak_kind}}
+    if not args.skip_e2e:
+        src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+        fwd = src < nb
+        hu = torch.from_numpy(src[fwd]).pin_memory()
+        hv = torch.from_numpy(nb[fwd]).pin_memory()
+        del src, fwd
+        times = []
+        for k in range(2):
+            flush_l2(k)
+            t0 = time.perf_counter()
+            g2 = rtr.Graph.from_edges(n, hu.numpy(), hv.numpy(), device=dev)
+            g2.count()
+            _, pv, _, _ = g2.weights(per_edge=False, support=False)
+            g2.close()
+            times.append(time.perf_counter() - t0)
+        sec = float(np.min(times))
+        out["e2e"] = {"value": m / sec, "unit": "edges/s", "h2d_bytes_per_step": 16 * m,
+                      "d2h_bytes_per_step": int(pv.nbytes) + 8, "ms_per_step": sec * 1e3}
+    return out
+
+
+def rmat_count_arm(args):
+    """--workload rmat_count: the config-3 counting line on its own (R-MAT at
+    --rmat-scale, rows layout unless --count-mode says otherwise)."""
+    import torch
+    torch.cuda.set_device(0)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda:0")
+
+    def flush_l2(k):
+        flush.fill_(k)
+        torch.cuda.synchronize(0)
+
+    peak, peak_kind = measured_peaks()
+    r = rmat24_leg(args, 0, flush_l2, peak, peak_kind, scale=args.rmat_scale, steps=args.steps, mode=args.count_mode)
+    line = {"metric": "counted edges/s (weighted triangle counting)", "value": r["edges_per_s"], "unit": "edges/s",
+            "n_gpus": 1, "steps": r["steps"], "warmup": 1, "ms_per_step": r["ms_per_count"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": r["workload"], "desc": r["desc"], "n": r["n"], "m": r["m"],
+                       "layout": r["layout"], "l2": "flushed (256 MiB write) before every step"},
+            "triangles": r["triangles"], "triangles_per_s": r["triangles_per_s"], "e2e": r.get("e2e"),
+            "roofline": r["roofline_count"], "gpu_launches": r["gpu_launches_per_count"] * r["steps"],
+            "kernel_ms": r["kernel_ms"], "generation_and_csr_build_ms": r["generation_and_csr_build_ms"]}
+    print(json.dumps(line), flush=True)
+
+
+def batched_leg(args, dev):
+    """The batched form's driver-measured ratio: the 4,096-graph SBM batch
+    (edge targets log-uniform in [1K, 200K], seeds 4000+i) as one decomposition
+    of the disjoint union against one plain decomposition per graph, both end
+    to end through the C ABI from host arrays."""
+    import rtrex_cuda_b200 as rtr
+    from rtrex_cuda_b200 import graphgen
+    t0 = time.perf_counter()
+    graphs = graphgen.sbm_batch(4096)
+    gen_s = time.perf_counter() - t0
+    K = len(graphs)
+    with rtr.Graph.batch(graphs, device=dev) as g:
+        tuning = g.autotune()
+    times, dev_ms = [], []
+    for k in range(3):  # one warm-up, two timed
+        t0 = time.perf_counter()
+        with rtr.Graph.batch(graphs, device=dev) as g:
+            g.set_tuning(*tuning)
+            g.decompose(args.eps)
+            counts = g.batch_cluster_counts()
+            dev_ms.append(g.kernel_ms()["decompose"])
+        if k:
+            times.append(time.perf_counter() - t0)
+    batched_s = float(np.mean(times))
+    t0 = time.perf_counter()
+    plain_counts = []
+    for (n, u, v) in graphs:
+        with rtr.Graph.from_edges(n, u, v, device=dev) as g1:
+            plain_counts.append(g1.decompose(args.eps))
+    plain_s = time.perf_counter() - t0
+    return {"workload": "sbm_batch", "graphs": K, "edges": int(sum(x[1].size for x in graphs)),
+            "batched_graphs_per_s": K / batched_s, "batched_device_graphs_per_s": K / (np.mean(dev_ms[1:]) / 1e3),
+            "plain_graphs_per_s": K / plain_s, "batched_vs_plain": plain_s / batched_s,
+            "per_graph_cluster_counts_equal": bool((np.asarray(plain_counts) == counts).all()),
+            "autotune": {"gallop_ratio": tuning[0], "heavy_degree": tuning[1], "heavy_edge": tuning[2]},
+            "generation_s": gen_s, "timing": "end to end through the C ABI from host arrays, mean of 2"}
+
+
+REF_CUDA_BIN = os.path.join(ROOT, "oracle", "_ref", "RTRex_CUDA")
+
+
+def gpu_baseline_leg(dev, timeout_s=240):
+    """The reference's CUDA port (RTRex_CUDA, built from its sources for sm_100a
+    by oracle/Makefile ref-cuda) on configs 1 and 2: its own phase timers, and how
+    its results diverge from the reference's sequential code (its outputs are not
+    a parity target: it skips triangles, breaks ties differently and defers
+    singletons)."""
+    from rtrex_cuda_b200 import graphgen
+    if not os.path.exists(REF_CUDA_BIN):
+        return {"unavailable": "oracle/_ref/RTRex_CUDA was not built (needs the reference sources)"}
+    import hashlib
+    gold_path = os.path.join(ROOT, "tests", "golden", "golden.json")
+    with open(gold_path) as f:
+        gold = json.load(f)["cases"]
+    out = {}
+    for name in ("gnp_cliques", "chung_lu"):
+        n, u, v = graphgen.config_graph(name)
+        res = {"n": n, "m": int(u.size)}
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "g.txt")
+            graphgen.write_escape(path, n, u, v)
+            t0 = time.perf_counter()
+            try:
+                r = subprocess.run([REF_CUDA_BIN, path, "g", repr(EPS), str(dev)], cwd=td, capture_output=True,
+                                   text=True, timeout=timeout_s)
+                stdout, rc = r.stdout, r.returncode
+            except subprocess.TimeoutExpired as e:
+                stdout = e.stdout.decode() if isinstance(e.stdout, bytes) else (e.stdout or "")
+                rc = None
+                res["timed_out_after_s"] = timeout_s
+            res["wall_s"] = time.perf_counter() - t0
+            res["rc"] = rc
+            grab = lambda pat: (lambda mm: float(mm.group(1)) if mm else None)(re.search(pat, stdout))
+            res["count_s"] = grab(r"\[GPU Triangle Count\] Found \d+ triangles in ([0-9.]+) s")
+            res["clean_s"] = grab(r"\[GPU Clean\] Done in ([0-9.]+) s")
+            res["extract_s"] = grab(r"\[Extraction\] \d+ clusters in ([0-9.]+) s")
+            tri = re.search(r"\[GPU Triangle Count\] Found (\d+) triangles", stdout)
+            ncl = re.search(r"\[Extraction\] (\d+) clusters", stdout)
+            res["triangles"] = int(tri.group(1)) if tri else None
+            res["clusters"] = int(ncl.group(1)) if ncl else None
+            want = gold[name]["0.3"]
+            res["triangles_reference_cpu"] = want["count"]["total"]
+            res["clusters_reference_cpu"] = want["extract"]["clusters"]
+            if rc == 0:
+                sec = sum(x for x in (res["count_s"], res["clean_s"], res["extract_s"]) if x)
+                res["edges_per_s"] = u.size / sec if sec else None
+                files = {}
+                for kind in ("decomposition", "stats", "freq", "cut"):
+                    fp = os.path.join(td, f"RTRex-CUDA-g-{kind}.txt")
+                    files[kind] = (os.path.exists(fp) and
+                                   hashlib.sha256(open(fp, "rb").read()).hexdigest() == want["files"][kind])
+                res["output_files_equal_reference_cpu"] = files
+        out[name] = res
+    return out
+
+
 def ours_arm(args):
     import torch
     import torch.distributed as dist
@@ -331,12 +535,14 @@ def ours_arm(args):
     torch.cuda.synchronize(dev)
     with ClockSampler(dev, not args.no_clocks) as clocks:
         wall0 = time.perf_counter()
+        count_ms = []
         for k in range(args.steps):
             flush_l2(k + 1)
             ncl = g.decompose(args.eps)
             km = g.kernel_ms()
             step_ms.append(km["decompose"])
             kms.append(km)
+            count_ms.append(g.stats()["ms_count"])
         torch.cuda.synchronize(dev)
         wall = time.perf_counter() - wall0
     barrier()
@@ -355,11 +561,13 @@ def ours_arm(args):
     b_count, orient_sum = count_bytes(n, off, nb)
     b_clean = clean_bytes(n, off, nb, status, total - left)
     peak, peak_kind = measured_peaks()
-    traffic = None
+    traffic, traffic_source = None, None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(dominant)
+            tj = json.load(f)
+        traffic = tj.get(dominant)
+        traffic_source = "profiles/traffic.json: " + tj.get("_captured", "ncu capture of an earlier build")
     if dominant == "k_clean_units":
         # the clean-replay stage timer: k_clean_rounds (large units, side stream)
         # with k_clean_units (small units) and the perVertex fold of the rounds
@@ -373,6 +581,7 @@ def ours_arm(args):
     roofline = {"kernel": label.get(dominant, dominant), "bound": "hbm", "achieved": achieved, "peak": peak,
                 "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "traffic_source": traffic_source,
                 "algorithmic_bytes": alg, "ms_per_launch": t_ms, "peak_kind": peak_kind}
     t_count = avg["k_edge_fold"] + avg["k_tri_fill"] + avg["k_vertex_fold"]
     roofline_count = {"kernels": "k_edge_fold+k_tri_fill+k_vertex_fold", "bound": "hbm",
@@ -410,6 +619,16 @@ def ours_arm(args):
                "seconds_per_run": sec}
 
     g.close()
+    t_count_stage = float(np.mean(count_ms)) / 1e3
+    extras = {}
+    if rank == 0 and world == 1 and not args.skip_extras:
+        for key, fn in (("config3_rmat24_count", lambda: rmat24_leg(args, dev, flush_l2, peak, peak_kind)),
+                        ("batched", lambda: batched_leg(args, dev)),
+                        ("gpu_baseline", lambda: gpu_baseline_leg(dev))):
+            try:
+                extras[key] = fn()
+            except Exception as e:  # a leg that cannot run is reported, not fatal
+                extras[key] = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -420,8 +639,10 @@ def ours_arm(args):
                        "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline, "roofline_count": roofline_count, "cpu_baseline": cpu,
             "gpu_launches": launches, "kernel_ms": avg, "wall_s_timed": wall,
+            "triangles": total, "triangles_per_s": total / t_count_stage, "count_stage_ms": t_count_stage * 1e3,
             "clocks": clocks.summary(),
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -593,6 +814,13 @@ def main():
         import torch.distributed as dist
         if dist.is_available() and dist.is_initialized():
             dist.destroy_process_group()
+        return
+    if args.workload == "rmat_count":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no counting-only entry point; "
+                              "its commonNbr at this scale runs for hours on the host"}), flush=True)
+            return
+        rmat_count_arm(args)
         return
     if args.impl == "reference":
         reference_arm(args)

@@ -63,6 +63,12 @@ def lib():
         L.orc_cells_vertex.restype = None
         L.orc_count_total.argtypes = [_i64, _i64p, _i64p]
         L.orc_count_total.restype = _i64
+        L.orc_nucleus.argtypes = [_i64, _i64p, _i64p]
+        L.orc_nucleus.restype = _i64
+        L.orc_nucleus_sizes.argtypes = [ctypes.POINTER(_i64)] * 3
+        L.orc_nucleus_sizes.restype = None
+        L.orc_nucleus_get.argtypes = [ctypes.c_void_p] * 11
+        L.orc_nucleus_get.restype = None
         L.orc_selfcheck_counts.argtypes = [ctypes.POINTER(_i64)] * 3
         L.orc_selfcheck_reset.argtypes = []
         _lib = L
@@ -253,3 +259,49 @@ def count_total(offsets: np.ndarray, nbors: np.ndarray) -> int:
     offsets = np.ascontiguousarray(offsets, np.int64)
     nbors = np.ascontiguousarray(nbors, np.int64) if len(nbors) else np.zeros(1, np.int64)
     return int(lib().orc_count_total(offsets.size - 1, offsets, nbors))
+
+
+@dataclass
+class Nuclei:
+    """Truss-hierarchy clusters in the order nucleus.cpp writes them."""
+    id: np.ndarray
+    c: np.ndarray
+    nv: np.ndarray
+    ne: np.ndarray
+    parent: np.ndarray
+    off: np.ndarray
+    vert: np.ndarray       # original labels
+    kappa: np.ndarray      # per slot of the relabelled CSR (-1 on backward slots)
+    rel_off: np.ndarray
+    rel_nb: np.ndarray
+    inverse: np.ndarray    # relabelled -> original
+    reference_overflow: int  # nonzero: the reference overruns a fixed array on this input (undefined output)
+
+    def text(self) -> str:
+        """The cluster file nucleus.cpp writes (nucleus.cpp:62-76)."""
+        out = []
+        for k in range(self.id.size):
+            out.append(f"Cluster id: {self.id[k]}, C: {self.c[k]}, n_vertices: {self.nv[k]}, "
+                       f"n_edges: {self.ne[k]}, parent: {self.parent[k]}\n")
+            out.append("".join(f"{x} " for x in self.vert[self.off[k]:self.off[k + 1]].tolist()) + "\n")
+        return "".join(out)
+
+
+def nucleus(c: "Csr") -> Nuclei:
+    """The nucleus path on the CSR (makeCSR + sortById) of a graph."""
+    L = lib()
+    k = int(L.orc_nucleus(c.n, c.offsets, _nb(c)))
+    nm, m2, ovf = _i64(), _i64(), _i64()
+    L.orc_nucleus_sizes(ctypes.byref(nm), ctypes.byref(m2), ctypes.byref(ovf))
+    a = {x: np.zeros(max(1, k), np.int64) for x in ("id", "c", "nv", "ne", "parent")}
+    off = np.zeros(k + 1, np.int64)
+    vert = np.zeros(max(1, nm.value), np.int64)
+    kappa = np.zeros(max(1, m2.value), np.int64)
+    rel_off = np.zeros(c.n + 1, np.int64)
+    rel_nb = np.zeros(max(1, m2.value), np.int64)
+    inverse = np.zeros(max(1, c.n), np.int64)
+    ptr = lambda x: x.ctypes.data
+    L.orc_nucleus_get(ptr(a["id"]), ptr(a["c"]), ptr(a["nv"]), ptr(a["ne"]), ptr(a["parent"]), ptr(off),
+                      ptr(vert), ptr(kappa), ptr(rel_off), ptr(rel_nb), ptr(inverse))
+    return Nuclei(a["id"][:k], a["c"][:k], a["nv"][:k], a["ne"][:k], a["parent"][:k], off, vert[:nm.value],
+                  kappa[:m2.value], rel_off, rel_nb[:m2.value], inverse[:c.n], int(ovf.value))

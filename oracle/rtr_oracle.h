@@ -13,6 +13,7 @@
  *   orc_extract        disjointExtract loop      Decomposition.h:566-919 (+ populateStats :473-491)
  *   orc_expand         expandClusters            Decomposition.h:958-1008
  *   orc_cells_*        commonNbr, cell by cell   Decomposition.h:70-115 (rtr_cells.cpp)
+ *   orc_nucleus        nucleus driver + nuclei   clustering/nucleus.cpp:12-81, Nucleus.h:125-565 (rtr_nucleus.cpp)
  *
  * Status bytes use the reference's characters: 'Y' alive, 'S' on the
  * deletion stack, 'N' deleted.  support[] is an integer companion the
@@ -76,6 +77,17 @@ void orc_cells_edge(int64_t n, const int64_t* offsets, const int64_t* nbors, int
 void orc_cells_vertex(int64_t n, const int64_t* offsets, const int64_t* nbors, int64_t k, const int64_t* verts,
                       double* perVertex);
 int64_t orc_count_total(int64_t n, const int64_t* offsets, const int64_t* nbors);
+
+/* The nucleus (truss-hierarchy) path, nucleus.cpp:12-81 (rtr_nucleus.cpp):
+ * returns the number of clusters; orc_nucleus_sizes / orc_nucleus_get copy
+ * the result out (clusters in output order with id, C, n_vertices, n_edges,
+ * parent and members in original labels; kappa per slot of the relabelled
+ * CSR; that CSR; new -> old labels; which of the reference's fixed-size
+ * arrays the input overruns, where the reference is undefined). */
+int64_t orc_nucleus(int64_t n, const int64_t* offsets, const int64_t* nbors);
+void orc_nucleus_sizes(int64_t* n_members, int64_t* m2, int64_t* overflow);
+void orc_nucleus_get(int64_t* id, int64_t* c, int64_t* nv, int64_t* ne, int64_t* parent, int64_t* voff,
+                     int64_t* vert, int64_t* kappa, int64_t* rel_off, int64_t* rel_nb, int64_t* inverse);
 
 /* Counters of the reference's self-checks that print and continue
  * (Decomposition.h:158-170 and :273-277), accumulated since the last reset. */

@@ -283,15 +283,16 @@ class Graph:
         _check(lib().rtr_get_csr(self._h, _ptr(off), _ptr(nb)))
         return off, nb[:2 * m]
 
-    def weights(self):
-        """(perEdge[2m], perVertex[n], support[2m], total)."""
+    def weights(self, per_edge: bool = True, support: bool = True):
+        """(perEdge[2m], perVertex[n], support[2m], total); per_edge / support
+        False skips reading those arrays back (None in their place)."""
         n, m = self.n, self.m
-        pe = np.zeros(max(1, 2 * m), np.float64)
+        pe = np.zeros(max(1, 2 * m), np.float64) if per_edge else None
         pv = np.zeros(max(1, n), np.float64)
-        sup = np.zeros(max(1, 2 * m), np.uint32)
+        sup = np.zeros(max(1, 2 * m), np.uint32) if support else None
         t = _i64()
         _check(lib().rtr_get_weights(self._h, _ptr(pe), _ptr(pv), _ptr(sup), ctypes.byref(t)))
-        return pe[:2 * m], pv[:n], sup[:2 * m], int(t.value)
+        return (pe[:2 * m] if per_edge else None), pv[:n], (sup[:2 * m] if support else None), int(t.value)
 
     def status(self) -> np.ndarray:
         m = self.m

@@ -21,7 +21,12 @@ regenerated from seeds (rtrex_cuda_b200.graphgen) or, for the bundled data
 files, the committed copies under tests/golden/data/ (``--copy-bundled``
 refreshes those copies, byte for byte, from the reference checkout first).
 
-Usage: python tests/golden/make_golden.py [--reference DIR] [--copy-bundled] [--expand-only]
+* nonsimple: the four files of ``RTRex <graph> g 0.3 s`` on a file with a repeated
+           and a reversed line, and on the same edges with the repeats dropped
+* nucleus: sha256 of the cluster file of the reference's ``nucleus <graph> <out>``
+           (clustering/nucleus.cpp) on every fixture graph
+
+Usage: python tests/golden/make_golden.py [--reference DIR] [--copy-bundled] [--expand-only] [--nonsimple-only] [--nucleus-only]
 (DIR defaults to $RTR_REFERENCE_DIR, else /root/reference; --expand-only
 recomputes only the expand entries of an existing golden.json)
 """
@@ -156,17 +161,79 @@ def add_expand(golden, dump_bin, cli_bin, reference):
             print("expand", name, eps, {t: e["nscores"] for t, e in entry["expand"].items()}, flush=True)
 
 
+# A file with a repeated line ("2 3" twice) and a reversed repeat ("1 0" after
+# "0 1"): loadGraph_Escape stores every line in both directions
+# (RTRex_Sequential/GraphIO.cpp:42-63) and makeCSR keeps repeated pairs
+# (Graph.cpp:344-384), so the reference decomposes a multigraph CSR.
+NONSIMPLE_TEXT = "5 8\n0 1\n1 2\n0 2\n2 3\n3 4\n2 4\n1 0\n2 3\n"
+
+
+def add_nonsimple(golden, cli_bin):
+    """The reference CLI's four files on NONSIMPLE_TEXT and on the same edge set
+    with the repeats dropped (what --simplify decomposes)."""
+    out = {"text": NONSIMPLE_TEXT, "eps": 0.3}
+    lines = NONSIMPLE_TEXT.strip().split("\n")
+    n = int(lines[0].split()[0])
+    pairs = sorted({tuple(sorted(map(int, ln.split()))) for ln in lines[1:]})
+    simple = f"{n} {len(pairs)}\n" + "".join(f"{a} {b}\n" for a, b in pairs)
+    for key, text in (("files", NONSIMPLE_TEXT), ("simplified_files", simple)):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "g.txt")
+            with open(path, "w") as f:
+                f.write(text)
+            subprocess.run([cli_bin, path, "g", "0.3", "s"], check=True, cwd=td, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL)
+            out[key] = {kind: sha(open(os.path.join(td, f"RTRex-g-{kind}.txt"), "rb").read())
+                        for kind in ("decomposition", "stats", "freq", "cut")}
+            if key == "files":
+                out["decomposition_text"] = open(os.path.join(td, "RTRex-g-decomposition.txt")).read()
+    golden["nonsimple"] = out
+
+
+def add_nucleus(golden, nucleus_bin):
+    """The reference nucleus driver (clustering/nucleus.cpp) on every fixture
+    graph: sha256 and line count of the cluster file it writes."""
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        for name in CASES:
+            path = case_path(name, td, None)
+            res = os.path.join(td, name + ".nuclei")
+            subprocess.run([nucleus_bin, path, res], check=True, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL, timeout=600)
+            data = open(res, "rb").read()
+            out[name] = {"sha": sha(data), "clusters": data.count(b"Cluster id:")}
+            print("nucleus", name, out[name]["clusters"], flush=True)
+    golden["nucleus"] = out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("RTR_REFERENCE_DIR", "/root/reference"))
     ap.add_argument("--copy-bundled", action="store_true")
     ap.add_argument("--expand-only", action="store_true")
+    ap.add_argument("--nonsimple-only", action="store_true")
+    ap.add_argument("--nucleus-only", action="store_true")
     args = ap.parse_args()
     if args.copy_bundled:
         copy_bundled(args.reference)
     dump_bin = os.path.join(ROOT, "oracle", "_ref", "rtr_ref_dump")
     cli_bin = os.path.join(ROOT, "oracle", "_ref", "RTRex")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.reference}"], check=True)
+    nucleus_bin = os.path.join(ROOT, "oracle", "_ref", "nucleus")
+    if args.nucleus_only:
+        with open(os.path.join(HERE, "golden.json")) as f:
+            golden = json.load(f)
+        add_nucleus(golden, nucleus_bin)
+        with open(os.path.join(HERE, "golden.json"), "w") as f:
+            json.dump(golden, f, indent=1, sort_keys=True)
+        return
+    if args.nonsimple_only:
+        with open(os.path.join(HERE, "golden.json")) as f:
+            golden = json.load(f)
+        add_nonsimple(golden, cli_bin)
+        with open(os.path.join(HERE, "golden.json"), "w") as f:
+            json.dump(golden, f, indent=1, sort_keys=True)
+        return
     if args.expand_only:
         with open(os.path.join(HERE, "golden.json")) as f:
             golden = json.load(f)
@@ -193,6 +260,8 @@ def main():
                 print(name, eps, res["count"]["total"], res["clean"]["total"], res["extract"]["clusters"], flush=True)
             golden["cases"][name] = entry
     add_expand(golden, dump_bin, cli_bin, args.reference)
+    add_nonsimple(golden, cli_bin)
+    add_nucleus(golden, nucleus_bin)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)
 
