@@ -142,6 +142,13 @@ int rtr_get_count_mode(const rtr_graph* g, int* mode, int* hub_degree, int* list
 int rtr_set_clean_split(rtr_graph* g, int64_t min_seeds, double max_mean_list);
 int rtr_get_clean_split(const rtr_graph* g, int64_t* min_seeds, double* max_mean_list);
 
+/* Split of the extraction: components of the cleaned graph with at least
+ * min_vertices vertices (default 512) replay their seed loop in a whole thread
+ * block -- the two-hop scan's pairs worked out by seven warps ahead of the warp
+ * that applies them in order -- and the others in one warp each.  Results are
+ * the same bits for every setting.  No counterpart in the reference. */
+int rtr_set_extract_split(rtr_graph* g, int64_t min_vertices);
+
 /* Bounds of the clean's device-side self-checks, to test their error reports
  * (no counterpart in the reference).  first_wait_rounds limits the first
  * bounded wait of the warp-per-unit replay on each window's asynchronous copies

@@ -110,6 +110,7 @@ def lib():
                                         ctypes.c_uint64, ctypes.c_int, P(_vp)]
     L.rtr_set_clean_split.argtypes = [_vp, _i64, ctypes.c_double]
     L.rtr_set_clean_checks.argtypes = [_vp, _i64, _i64]
+    L.rtr_set_extract_split.argtypes = [_vp, _i64]
     L.rtr_get_clean_split.argtypes = [_vp, P(_i64), P(ctypes.c_double)]
     L.rtr_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, _i64, ctypes.c_int, P(_vp)]
     L.rtr_server_add_graph.argtypes = [_vp, _vp, _vp, _i64, _i64, ctypes.c_int, P(_i64)]
@@ -359,6 +360,11 @@ class Graph:
         most `max_mean_list` entries on average replay in parallel rounds (one
         thread block each), the others one warp per unit (same bits)."""
         _check(lib().rtr_set_clean_split(self._h, int(min_seeds), float(max_mean_list)))
+
+    def set_extract_split(self, min_vertices: int = 512):
+        """Components of at least min_vertices vertices are extracted by a thread
+        block each, the others by a warp each (same bits)."""
+        _check(lib().rtr_set_extract_split(self._h, int(min_vertices)))
 
     def set_clean_checks(self, first_wait_rounds: int = 0, stack_entries: int = -1):
         """Lower the clean's device-side check bounds (to test their error reports)."""

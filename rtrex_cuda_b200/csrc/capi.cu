@@ -410,6 +410,16 @@ int rtr_set_clean_checks(rtr_graph* g, int64_t first_wait_rounds, int64_t stack_
     return RTR_OK;
 }
 
+int rtr_set_extract_split(rtr_graph* g, int64_t min_vertices)
+{
+    if (!g || min_vertices < 2) {
+        set_error("rtr_set_extract_split: null graph or min_vertices below 2");
+        return RTR_ERR_ARG;
+    }
+    g->extract_big = min_vertices;
+    return RTR_OK;
+}
+
 int rtr_get_clean_split(const rtr_graph* g, int64_t* min_seeds, double* max_mean_list)
 {
     if (!g || !min_seeds || !max_mean_list) {

@@ -24,12 +24,13 @@
 //                  every lane binary-searching its element in the longer one,
 //                  and folds the hits in lane order (ascending z)
 //   k_rows_hub     a thread block per vertex of degree >= hub, hubs in
-//                  descending degree: the block's 8 warps take 8 consecutive y
-//                  at once, searching x's row through a shared-memory sample of
-//                  it (every stride-th element) and a one-window global search;
-//                  each warp writes its y's z > y weights, in order, to its own
-//                  buffer, and warp 0 then folds the 8 buffers in y order --
-//                  only the perVertex chain itself is sequential.
+//                  descending degree: 7 producer warps take 7 consecutive y at
+//                  once, searching x's row through a shared-memory sample of it
+//                  (every stride-th element) and a one-window global search;
+//                  each writes its y's z > y weights, in order, to its own
+//                  buffer, which warp 0 folds in y order while the producers
+//                  work on the next 7 (double-buffered) -- only the perVertex
+//                  chain itself is sequential.
 // The hub kernel runs on the graph's second stream, concurrently with the
 // other two (it holds the longest dependent chain: ~10^8 adds for the largest
 // R-MAT scale-24 hub).
@@ -131,17 +132,21 @@ __global__ void __launch_bounds__(kMediumBlock) k_rows_medium(RowsArgs a)
     }
 }
 
-// Hubs: hubs[] in descending degree; buf holds kHubWarps regions of cap
-// doubles per block (cap >= the largest hub degree, which bounds the z > y
-// hits of one y).
+// Hubs: hubs[] in descending degree.  Warp 0 of the block folds perVertex;
+// warps 1..kHubWarps-1 produce: round r gives them the next kHubWarps-1
+// consecutive y, each writing its y's z > y weights in order to its own region
+// of buffer set r&1 (buf holds 2 x (kHubWarps-1) regions of cap doubles per
+// block; cap >= the largest hub degree bounds the hits of one y), while warp 0
+// folds round r-1 from the other set.  One block barrier per round.
 __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_t* __restrict__ hubs, int64_t nhub,
                                                          double* __restrict__ buf, int64_t cap)
 {
+    constexpr int P = kHubWarps - 1;  // producer warps
     __shared__ int32_t s_idx[kHubIndexMax];
     __shared__ double s_w[kHubWarps][32];
-    __shared__ int64_t s_len[kHubWarps];
+    __shared__ int64_t s_len[2][P];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double* region = buf + ((int64_t)blockIdx.x * kHubWarps + wib) * cap;
+    auto region = [&](int set, int w) { return buf + (((int64_t)blockIdx.x * 2 + set) * P + w) * cap; };
     for (int64_t h = blockIdx.x; h < nhub; h += gridDim.x) {
         const int32_t x = hubs[h];
         const int dx = a.deg[x];
@@ -165,10 +170,10 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
             return lower_bound_row(a.nb, w0, w1, v);
         };
         auto search_g = [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(a.nb, lo, hi, v); };
-        double pvacc = 0.0;  // meaningful in warp 0
-        for (int64_t base = a0; base < a1; base += kHubWarps) {
-            const int64_t i = base + wib;
+        // producer warp w (1..P) on slot i: y's z > y weights into region(set, w-1)
+        auto produce = [&](int64_t i, int set) {
             int64_t len = 0;
+            double* reg = region(set, wib - 1);
             if (i < a1) {  // uniform across the warp
                 const int32_t y = a.nb[i];
                 const int dy = a.deg[y];
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
                     const int below = owner ? __popc(__ballot_sync(0xffffffffu, hit && z < y)) : 0;
                     const int rank = __popc(mask & ((1u << lane) - 1u));
                     if (owner) fold_hits(hit, w, s_w[wib], lane, &peacc, nullptr, 0);
-                    if (hit && rank >= below) region[len + rank - below] = w;
+                    if (hit && rank >= below) reg[len + rank - below] = w;
                     len += cnt - below;
                 };
                 if (B1 - B0 <= A1 - A0) {
@@ -197,15 +202,21 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
                 }
                 if (owner && lane == 0) a.pe[i] = peacc;
             }
-            if (lane == 0) s_len[wib] = len;
-            __syncthreads();
+            if (lane == 0) s_len[set][wib - 1] = len;
+        };
+        double pvacc = 0.0;  // meaningful in warp 0
+        const int64_t rounds = (d + P - 1) / P;
+        if (wib > 0) produce(a0 + wib - 1, 0);
+        __syncthreads();
+        for (int64_t r = 0; r < rounds; ++r) {
+            const int set = (int)(r & 1);
             if (wib == 0) {
-                for (int w = 0; w < kHubWarps; ++w) {
-                    const int64_t L = s_len[w];
-                    const double* r = buf + ((int64_t)blockIdx.x * kHubWarps + w) * cap;
-                    double v = lane < L ? r[lane] : 0.0;
+                for (int w = 0; w < P; ++w) {
+                    const int64_t L = s_len[set][w];
+                    const double* rg = region(set, w);
+                    double v = lane < L ? rg[lane] : 0.0;
                     for (int64_t k0 = 0; k0 < L; k0 += 32) {
-                        const double vn = k0 + 32 + lane < L ? r[k0 + 32 + lane] : 0.0;  // next 32, ahead of the chain
+                        const double vn = k0 + 32 + lane < L ? rg[k0 + 32 + lane] : 0.0;  // next 32, ahead of the chain
                         const int c = L - k0 < 32 ? (int)(L - k0) : 32;
                         double t[32];
 #pragma unroll
@@ -216,6 +227,8 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
                         v = vn;
                     }
                 }
+            } else if (r + 1 < rounds) {
+                produce(a0 + (r + 1) * P + wib - 1, set ^ 1);
             }
             __syncthreads();
         }
@@ -283,7 +296,7 @@ int count_rows(rtr_graph* g, Scratch& sc)
         int dev_sms = 148;
         cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device);
         hub_grid = (int)((int64_t)nh < dev_sms ? (int64_t)nh : dev_sms);
-        hbuf = (double*)sc.get(sizeof(double) * (size_t)hub_grid * kHubWarps * (size_t)(cap + 32));
+        hbuf = (double*)sc.get(sizeof(double) * (size_t)hub_grid * 2 * (kHubWarps - 1) * (size_t)(cap + 32));
         if (!hbuf) {
             set_error("device allocation failed (hub fold buffers, %lld hubs of degree up to %lld)", (long long)nh,
                       (long long)cap);

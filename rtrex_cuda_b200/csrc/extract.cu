@@ -167,16 +167,18 @@ __global__ void k_comp_sizes(CompDesc* __restrict__ comps, int64_t nc, int64_t n
 
 __global__ void k_comp_finish(CompDesc* __restrict__ comps, int64_t nc, const int64_t* __restrict__ boff,
                               const int64_t* __restrict__ soff, const int64_t* __restrict__ sneed,
-                              uint64_t* __restrict__ order_keys)
+                              uint64_t* __restrict__ order_keys, int64_t big_thr)
 {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         comps[c].bbase = boff[c];
         comps[c].sbase = soff[c];
         comps[c].scap = sneed[c];
-        // largest components first
+        // components for the block kernel (at least big_thr vertices) first, then
+        // the others; largest first within each group
         const int64_t wr = comps[c].vcount + sneed[c];
-        const uint64_t w = (uint64_t)(wr < 0xffffffffll ? wr : 0xffffffffll);
-        order_keys[c] = ((uint64_t)(0xffffffffu - (uint32_t)w) << 32) | (uint64_t)c;
+        const uint64_t w = (uint64_t)(wr < 0x7fffffffll ? wr : 0x7fffffffll);
+        const uint64_t small = comps[c].vcount >= big_thr ? 0u : 1u;
+        order_keys[c] = (small << 63) | ((uint64_t)(0x7fffffffu - (uint32_t)w) << 32) | (uint64_t)c;
     }
 }
 
@@ -373,6 +375,238 @@ __device__ void sort_ids(int32_t* x, int64_t n)
     }
 }
 
+// Per-component state of the seed loop: the scratch regions of the component
+// and lane 0's containers (the member set, the output cursor, the cluster count).
+struct CompCtx {
+    int64_t vb, nv;
+    int32_t base;  // graph-local id offset in a batch (the member set hashes local ids)
+    int32_t* ukey;
+    int32_t* unext;
+    int32_t* ubucket;
+    int32_t* twohop;
+    Cand* cand;
+    DelEntry* dstack;
+    int64_t scap;
+    int64_t out;   // lane 0
+    int32_t ncl;   // lane 0
+    UsetOrder S;   // lane 0
+};
+
+__device__ __forceinline__ CompCtx comp_ctx(const ExtractArgs& a, const CompDesc& cd)
+{
+    CompCtx cc;
+    cc.vb = cd.vbegin;
+    cc.nv = cd.vcount;
+    cc.base = a.vbase ? a.vbase[a.vlist[cd.vbegin]] : 0;
+    cc.ukey = a.ukey + cd.vbegin;
+    cc.unext = a.unext + cd.vbegin;
+    cc.ubucket = a.ubucket + cd.bbase;
+    cc.twohop = a.twohop + cd.vbegin;
+    cc.cand = a.cand + cd.vbegin;
+    cc.dstack = a.dstack + cd.sbase;
+    cc.scap = cd.scap;
+    cc.out = cd.vbegin;
+    cc.ncl = 0;
+    return cc;
+}
+
+// Lane 0: the seed's cluster starts as {u} plus its alive neighbours, in row
+// order (Decomposition.h:587-620), each marked clustered and in nbdBitMap.
+__device__ __forceinline__ void seed_members(const ExtractArgs& a, CompCtx& cc, int32_t u)
+{
+    cc.S.init(cc.ukey, cc.unext, cc.ubucket);
+    cc.S.insert(u - cc.base);
+    a.clustered[u] = 1;
+    for (int64_t j = a.off[u]; j < a.off[u + 1]; ++j) {
+        if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
+        const int32_t v = a.nb[j];
+        cc.S.insert(v - cc.base);
+        a.nbd[v] = 1;
+        a.clustered[v] = 1;
+    }
+}
+
+// The two-hop scan of seed u (Decomposition.h:728-805) by one warp: for each
+// pair (v, w) of the seed's alive neighbours of degree <= du/eps (w from v on,
+// w == v included), the rows of the lower-degree one are taken 32 candidates x
+// at a time: within one pair every x is distinct, so each lane updates its own
+// triwgt[x] / in2hop[x], and the one shared sum (internal) is folded in lane
+// order, i.e. in the reference's order, identically on every lane.
+__device__ void two_hop_warp(const ExtractArgs& a, CompCtx& cc, int32_t u, double* sw, double* internal_out,
+                             int64_t* n2_out)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t du = a.deg[u];
+    const int64_t r0 = a.off[u], r1 = a.off[u + 1];
+    double internal = 0;  // the same value on every lane
+    int64_t n2 = 0;       // likewise
+    const double thr = (double)du / a.eps;
+    for (int64_t j = r0; j < r1; ++j) {
+        if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
+        const int32_t v = a.nb[j];
+        const int64_t dv = a.deg[v];
+        if ((double)dv > thr) continue;
+        for (int64_t k = j; k < r1; ++k) {  // k starts at j: w == v included
+            if (a.st[fwd_slot(u, k, a.nb, a.partner)] == ST_N) continue;
+            const int32_t w = a.nb[k];
+            const int64_t dw = a.deg[w];
+            if ((double)dw > thr) continue;
+            internal += 1.0 / (double)(du * dv * dw);
+            const int32_t lower = (dv < dw) ? v : w;
+            const int32_t higher = (dv < dw) ? w : v;
+            const int64_t l1 = a.off[lower + 1];
+            for (int64_t lb = a.off[lower]; lb < l1; lb += 32) {
+                const int64_t l = lb + lane;
+                bool ok = false, in_nbd = false;
+                int32_t x = 0;
+                double wgt = 0.0;
+                if (l < l1 && a.st[fwd_slot(lower, l, a.nb, a.partner)] != ST_N) {
+                    x = a.nb[l];
+                    if (x != lower && x != higher && x != u) {
+                        const int64_t lh = find_slot(a.off, a.nb, higher, x);
+                        if (lh >= 0 && a.st[fwd_slot(higher, lh, a.nb, a.partner)] != ST_N) {
+                            ok = true;
+                            wgt = 1.0 / (double)((int64_t)a.deg[x] * dv * dw);
+                            in_nbd = a.nbd[x] != 0;
+                        }
+                    }
+                }
+                // candidates inside the neighbourhood feed internal, in order
+                const bool inner = ok && in_nbd && x > v && x > w;
+                const unsigned im = __ballot_sync(0xffffffffu, inner);
+                if (im) {
+                    if (inner) sw[__popc(im & lt)] = wgt;
+                    __syncwarp();
+                    const int ni = __popc(im);
+                    for (int q = 0; q < ni; ++q) internal += sw[q];
+                }
+                // the others are two-hop candidates: distinct x, one lane each
+                bool fresh = false;
+                if (ok && !in_nbd) {
+                    fresh = !a.in2hop[x];
+                    if (fresh) a.in2hop[x] = 1;
+                    a.triwgt[x] += wgt;
+                }
+                const unsigned fm = __ballot_sync(0xffffffffu, fresh);
+                if (fresh) cc.twohop[n2 + __popc(fm & lt)] = x;
+                n2 += __popc(fm);
+                __syncwarp();  // the next chunk or pair may touch the same x from another lane
+            }
+        }
+    }
+    *internal_out = internal;
+    *n2_out = n2;
+}
+
+// Lane 0: rank the two-hop candidates (std::set order, then the reference's
+// unstable sort by weight, Decomposition.h:811-829), take the best prefix by
+// the ratio (:847-864), clear the neighbour bits, and write the cluster out.
+// Returns nonzero when the clusters would not partition the component.
+__device__ int seed_select(const ExtractArgs& a, CompCtx& cc, int32_t u, double internal, int64_t n2,
+                           int32_t* ncl_members)
+{
+    sort_ids(cc.twohop, n2);
+    double potential = 0;
+    for (int64_t k = 0; k < n2; ++k) {
+        const int32_t x = cc.twohop[k];
+        cc.cand[k].vertex = x;
+        cc.cand[k].pad = 0;
+        cc.cand[k].wgt = a.triwgt[x];
+        potential += a.triwgt[x];
+        a.triwgt[x] = 0;
+        a.in2hop[x] = 0;
+    }
+    introsort(cc.cand, cc.cand + n2, [](const Cand& p, const Cand& q) { return p.wgt > q.wgt; });
+    double ratio = internal / (internal + potential);
+    int64_t maxind = -1;
+    double num = 0, den = 0;
+    for (int64_t k = 0; k < n2; ++k) {
+        num += cc.cand[k].wgt;
+        den += a.pv[cc.cand[k].vertex];
+        const double nr = (internal + num) / (internal + potential + den);
+        if (nr > ratio) {
+            ratio = nr;
+            maxind = k;
+        }
+    }
+    for (int64_t k = 0; k <= maxind; ++k) {
+        cc.S.insert(cc.cand[k].vertex - cc.base);
+        a.clustered[cc.cand[k].vertex] = 1;
+    }
+    // The reference clears the bit of every neighbour of u (Decomposition.h:879-883).
+    // Only the alive ones were set, and a dead neighbour may belong to another
+    // component that a different thread is processing right now, so clear
+    // exactly the bits this seed set.
+    for (int64_t j = a.off[u]; j < a.off[u + 1]; ++j)
+        if (a.st[fwd_slot(u, j, a.nb, a.partner)] != ST_N) a.nbd[a.nb[j]] = 0;
+    if (cc.out + cc.S.size > cc.vb + cc.nv || cc.ncl >= cc.nv) {  // clusters must partition the component
+        atomicOr(a.err, (unsigned)DEV_ERR_SCRATCH);
+        return 1;
+    }
+    a.hdr_seed[cc.vb + cc.ncl] = u;
+    a.hdr_start[cc.vb + cc.ncl] = cc.out;
+    a.hdr_size[cc.vb + cc.ncl] = cc.S.size;
+    *ncl_members = cc.S.size;
+    for (int32_t p = cc.S.head; p != -1; p = cc.S.next[p]) a.out_vert[cc.out++] = cc.S.key[p] + cc.base;
+    ++cc.ncl;
+    return 0;
+}
+
+// The whole warp: the deletion stack -- every still-'Y' edge of the cluster's
+// members, members in set-iteration order (the list lane 0 just wrote to
+// out_vert, nm entries ending at out_end) and each member's row in order, 32
+// row entries at a time; an edge between two members is pushed from the first
+// member's row only ('S' afterwards) -- then the cascade that follows.
+__device__ void seed_delete(const ExtractArgs& a, CompCtx& cc, int32_t nm, int64_t out_end, double* sw)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t mbase = out_end - nm;
+    int64_t top = 0;
+    bool full = false;
+    for (int32_t q = 0; q < nm && !full; ++q) {
+        const int32_t z = a.out_vert[mbase + q];
+        const int64_t j1 = a.off[z + 1];
+        for (int64_t jb = a.off[z]; jb < j1; jb += 32) {
+            const int64_t j = jb + lane;
+            int64_t f = -1;
+            bool push = false;
+            if (j < j1) {
+                f = fwd_slot(z, j, a.nb, a.partner);
+                push = a.st[f] == ST_Y;
+            }
+            const unsigned pm = __ballot_sync(0xffffffffu, push);
+            const int np = __popc(pm);
+            if (top + np > cc.scap) {
+                if (lane == 0) atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+                full = true;  // stop scanning; the cascade still runs on what was pushed
+                break;
+            }
+            if (push) {
+                cc.dstack[top + __popc(pm & lt)] = DelEntry{(int32_t)f, z, a.nb[j], 0};
+                a.st[f] = ST_S;
+            }
+            top += np;
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    delete_and_clean_warp(a, cc.dstack, top, cc.scap, sw);
+}
+
+// A component of one vertex: a singleton cluster with no edges to delete.
+__device__ __forceinline__ void singleton_component(const ExtractArgs& a, const CompDesc& cd, int64_t c)
+{
+    const int32_t u = a.vlist[cd.vbegin];
+    a.clustered[u] = 1;
+    a.hdr_seed[cd.vbegin] = u;
+    a.hdr_start[cd.vbegin] = cd.vbegin;
+    a.hdr_size[cd.vbegin] = 1;
+    a.out_vert[cd.vbegin] = u;
+    a.ncl[c] = 1;
+}
+
 constexpr int kExtractBlock = 128;
 
 __global__ void __launch_bounds__(kExtractBlock) k_extract_components(ExtractArgs a, const CompDesc* __restrict__ comps,
@@ -380,16 +614,12 @@ __global__ void __launch_bounds__(kExtractBlock) k_extract_components(ExtractArg
                                                             unsigned* __restrict__ next_comp)
 {
     // One warp per component.  Lane 0 replays the seed loop's sequential parts
-    // (the member set, the candidate ranking, the deletion cascade); the
-    // two-hop scan -- for each pair (v, w) of the seed's neighbours, the rows of
-    // the lower-degree one -- is taken 32 candidates x at a time by the whole
-    // warp: within one pair every x is distinct, so each lane updates its own
-    // triwgt[x] / in2hop[x], and the one shared sum (internal) is folded in
-    // lane order, i.e. in the reference's order, identically on every lane.
-    // (Giving each thread its own component would put the largest components,
-    // which are handed out first, into the same warp and serialise them.)
+    // (the member set, the candidate ranking, the deletion cascade's
+    // bookkeeping); the two-hop scan and the deletion stack are taken 32 at a
+    // time by the whole warp.  (Giving each thread its own component would put
+    // the largest components, which are handed out first, into the same warp
+    // and serialise them.)
     const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
     __shared__ double s_fold[kExtractBlock / 32][32];
     double* sw = s_fold[threadIdx.x >> 5];
     while (true) {
@@ -399,201 +629,208 @@ __global__ void __launch_bounds__(kExtractBlock) k_extract_components(ExtractArg
         if ((int64_t)ci >= nc) return;
         const int64_t c = (int64_t)(uint32_t)order[ci];
         const CompDesc cd = comps[c];
-        const int64_t vb = cd.vbegin, nv = cd.vcount;
-        if (nv == 1) {  // an isolated vertex: a singleton cluster with no edges to delete
-            if (lane == 0) {
-                const int32_t u = a.vlist[vb];
-                a.clustered[u] = 1;
-                a.hdr_seed[vb] = u;
-                a.hdr_start[vb] = vb;
-                a.hdr_size[vb] = 1;
-                a.out_vert[vb] = u;
-                a.ncl[c] = 1;
-            }
+        if (cd.vcount == 1) {
+            if (lane == 0) singleton_component(a, cd, c);
             continue;
         }
-        // The member set hashes vertex ids; in a batch the ids are offset per
-        // graph, so the set works on graph-local ids to iterate as the graph
-        // alone would.
-        const int32_t base = a.vbase ? a.vbase[a.vlist[vb]] : 0;
-        int32_t* ukey = a.ukey + vb;
-        int32_t* unext = a.unext + vb;
-        int32_t* ubucket = a.ubucket + cd.bbase;
-        int32_t* twohop = a.twohop + vb;
-        Cand* cand = a.cand + vb;
-        DelEntry* dstack = a.dstack + cd.sbase;
-        int64_t out = vb;   // lane 0
-        int32_t ncl = 0;    // lane 0
-        UsetOrder S;        // lane 0
-        for (int64_t idx = 0; idx < nv; ++idx) {
+        CompCtx cc = comp_ctx(a, cd);
+        for (int64_t idx = 0; idx < cc.nv; ++idx) {
             __syncwarp();  // lane 0's writes of the previous seed are visible
-            const int32_t u = a.vlist[vb + idx];
+            const int32_t u = a.vlist[cc.vb + idx];
             if (a.clustered[u]) continue;
-            const int64_t du = a.deg[u];
-            const int64_t r0 = a.off[u], r1 = a.off[u + 1];
-            if (lane == 0) {
-                S.init(ukey, unext, ubucket);
-                S.insert(u - base);
-                a.clustered[u] = 1;
-                for (int64_t j = r0; j < r1; ++j) {
-                    if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
-                    const int32_t v = a.nb[j];
-                    S.insert(v - base);
-                    a.nbd[v] = 1;
-                    a.clustered[v] = 1;
-                }
-            }
+            if (lane == 0) seed_members(a, cc, u);
             __syncwarp();
-            double internal = 0;  // the same value on every lane
-            int64_t n2 = 0;       // likewise
+            double internal = 0;
+            int64_t n2 = 0;
+            two_hop_warp(a, cc, u, sw, &internal, &n2);
+            int fail = 0;
+            int32_t nm = 0;
+            if (lane == 0) fail = seed_select(a, cc, u, internal, n2, &nm);
+            __syncwarp();
+            if (__shfl_sync(0xffffffffu, fail, 0)) break;
+            seed_delete(a, cc, __shfl_sync(0xffffffffu, nm, 0), __shfl_sync(0xffffffffu, cc.out, 0), sw);
+        }
+        if (lane == 0) a.ncl[c] = cc.ncl;
+    }
+}
+
+// Large components, one thread block each.  The seed loop is the warp kernel's
+// (warp 0 runs it), except for the two-hop scan: the block's other warps work
+// out, seven pairs (v, w) ahead, each pair's candidates x in row order -- alive,
+// in both rows, not u/v/w -- with their weights and whether x is in the
+// neighbourhood, into per-warp buffers; warp 0 then applies the pairs in the
+// reference's order: internal += 1/(du dv dw), internal += the in-neighbourhood
+// candidates' weights (x > v, w) in row order, triwgt[x] += weight for the
+// others (distinct x within a pair: one lane each).  Double-buffered: warp 0
+// applies round r while the producers fill round r+1, one block barrier per
+// round.  Every floating-point operation is the warp kernel's, in its order.
+constexpr int kBigWarps = 8;
+constexpr int kBigBlock = 32 * kBigWarps;
+
+struct PairHit {
+    int32_t x;
+    int32_t inner;  // 1: in the neighbourhood and x > v, w (feeds internal); 2: in it, not counted; 0: two-hop
+    double w;
+};
+
+__global__ void __launch_bounds__(kBigBlock) k_extract_big(ExtractArgs a, const CompDesc* __restrict__ comps,
+                                                            const uint64_t* __restrict__ order, int64_t nbig,
+                                                            unsigned* __restrict__ next_big, int32_t* __restrict__ fbuf,
+                                                            PairHit* __restrict__ hbuf, int64_t hcap)
+{
+    constexpr int P = kBigWarps - 1;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    __shared__ double s_fold[kBigWarps][32];
+    __shared__ int64_t s_cnt[2][P];
+    __shared__ int64_t s_pv[2][P], s_pw[2][P];  // the pair's (dv, dw)
+    __shared__ unsigned s_ci;
+    __shared__ int64_t s_nf;
+    __shared__ int s_fail;
+    double* sw = s_fold[wib];
+    int32_t* flist = fbuf + (int64_t)blockIdx.x * hcap;  // the seed's alive neighbours of degree <= du/eps
+    auto hits = [&](int set, int w) { return hbuf + (((int64_t)blockIdx.x * 2 + set) * P + w) * hcap; };
+    while (true) {
+        if (threadIdx.x == 0) s_ci = atomicAdd(next_big, 1u);
+        __syncthreads();
+        const unsigned ci = s_ci;
+        __syncthreads();
+        if ((int64_t)ci >= nbig) return;
+        const int64_t c = (int64_t)(uint32_t)order[ci];
+        const CompDesc cd = comps[c];
+        CompCtx cc = comp_ctx(a, cd);
+        for (int64_t idx = 0; idx < cc.nv; ++idx) {
+            const int32_t u = a.vlist[cc.vb + idx];
+            __syncthreads();  // warp 0's writes of the previous seed are visible
+            if (a.clustered[u]) continue;  // uniform: every thread reads it after the barrier
+            const int64_t du = a.deg[u];
             const double thr = (double)du / a.eps;
-            for (int64_t j = r0; j < r1; ++j) {
-                if (a.st[fwd_slot(u, j, a.nb, a.partner)] == ST_N) continue;
-                const int32_t v = a.nb[j];
-                const int64_t dv = a.deg[v];
-                if ((double)dv > thr) continue;
-                for (int64_t k = j; k < r1; ++k) {  // k starts at j: w == v included
-                    if (a.st[fwd_slot(u, k, a.nb, a.partner)] == ST_N) continue;
-                    const int32_t w = a.nb[k];
-                    const int64_t dw = a.deg[w];
-                    if ((double)dw > thr) continue;
-                    internal += 1.0 / (double)(du * dv * dw);
-                    const int32_t lower = (dv < dw) ? v : w;
-                    const int32_t higher = (dv < dw) ? w : v;
+            if (wib == 0) {
+                if (lane == 0) seed_members(a, cc, u);
+                __syncwarp();
+                // the pair list's vertices: alive neighbours within the degree bound, row order
+                int64_t nf = 0;
+                const int64_t r1 = a.off[u + 1];
+                for (int64_t jb = a.off[u]; jb < r1; jb += 32) {
+                    const int64_t j = jb + lane;
+                    bool keep = false;
+                    int32_t v = 0;
+                    if (j < r1 && a.st[fwd_slot(u, j, a.nb, a.partner)] != ST_N) {
+                        v = a.nb[j];
+                        keep = !((double)a.deg[v] > thr);
+                    }
+                    const unsigned km = __ballot_sync(0xffffffffu, keep);
+                    if (keep) flist[nf + __popc(km & lt)] = v;
+                    nf += __popc(km);
+                }
+                if (lane == 0) s_nf = nf;
+            }
+            __syncthreads();
+            const int64_t nf = s_nf;
+            const int64_t npairs = nf * (nf + 1) / 2;
+            const int64_t rounds = (npairs + P - 1) / P;
+            // producer warp w (1..P): pair number p, in (j, k >= j) order, into set
+            auto produce = [&](int64_t p, int set) {
+                const int w = wib - 1;
+                int64_t cnt = 0, dvv = 0, dww = 0;
+                if (p < npairs) {
+                    // row j holds pairs (j, j..nf-1): find j with p in [S(j), S(j+1)), S(j) = j*nf - j(j-1)/2
+                    int64_t lo = 0, hi = nf - 1;
+                    while (lo < hi) {
+                        const int64_t mid = (lo + hi + 1) >> 1;
+                        if (mid * nf - mid * (mid - 1) / 2 <= p) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    const int64_t j = lo, k = j + (p - (j * nf - j * (j - 1) / 2));
+                    const int32_t v = flist[j];
+                    const int32_t x2 = flist[k];
+                    dvv = a.deg[v];
+                    dww = a.deg[x2];
+                    const int32_t lower = (dvv < dww) ? v : x2;
+                    const int32_t higher = (dvv < dww) ? x2 : v;
+                    PairHit* out = hits(set, w);
                     const int64_t l1 = a.off[lower + 1];
                     for (int64_t lb = a.off[lower]; lb < l1; lb += 32) {
                         const int64_t l = lb + lane;
-                        bool ok = false, in_nbd = false;
-                        int32_t x = 0;
-                        double wgt = 0.0;
+                        bool ok = false;
+                        PairHit hh{0, 0, 0.0};
                         if (l < l1 && a.st[fwd_slot(lower, l, a.nb, a.partner)] != ST_N) {
-                            x = a.nb[l];
+                            const int32_t x = a.nb[l];
                             if (x != lower && x != higher && x != u) {
                                 const int64_t lh = find_slot(a.off, a.nb, higher, x);
                                 if (lh >= 0 && a.st[fwd_slot(higher, lh, a.nb, a.partner)] != ST_N) {
                                     ok = true;
-                                    wgt = 1.0 / (double)((int64_t)a.deg[x] * dv * dw);
-                                    in_nbd = a.nbd[x] != 0;
+                                    const bool in_nbd = a.nbd[x] != 0;
+                                    hh.x = x;
+                                    hh.w = 1.0 / (double)((int64_t)a.deg[x] * dvv * dww);
+                                    hh.inner = in_nbd ? ((x > v && x > x2) ? 1 : 2) : 0;
                                 }
                             }
                         }
-                        // candidates inside the neighbourhood feed internal, in order
-                        const bool inner = ok && in_nbd && x > v && x > w;
-                        const unsigned im = __ballot_sync(0xffffffffu, inner);
-                        if (im) {
-                            if (inner) sw[__popc(im & lt)] = wgt;
+                        const unsigned om = __ballot_sync(0xffffffffu, ok);
+                        if (ok) out[cnt + __popc(om & lt)] = hh;
+                        cnt += __popc(om);
+                    }
+                }
+                if (lane == 0) {
+                    s_cnt[set][w] = cnt;
+                    s_pv[set][w] = dvv;
+                    s_pw[set][w] = dww;
+                }
+            };
+            double internal = 0;  // warp 0, the same on every lane
+            int64_t n2 = 0;
+            if (wib > 0) produce(wib - 1, 0);
+            __syncthreads();
+            for (int64_t r = 0; r < rounds; ++r) {
+                const int set = (int)(r & 1);
+                if (wib == 0) {
+                    for (int w = 0; w < P && r * P + w < npairs; ++w) {
+                        internal += 1.0 / (double)(du * s_pv[set][w] * s_pw[set][w]);
+                        const PairHit* in = hits(set, w);
+                        const int64_t cnt = s_cnt[set][w];
+                        for (int64_t b = 0; b < cnt; b += 32) {
+                            const bool valid = b + lane < cnt;
+                            PairHit hh{0, 2, 0.0};
+                            if (valid) hh = in[b + lane];
+                            const bool inner = valid && hh.inner == 1;
+                            const unsigned im = __ballot_sync(0xffffffffu, inner);
+                            if (im) {
+                                if (inner) sw[__popc(im & lt)] = hh.w;
+                                __syncwarp();
+                                const int ni = __popc(im);
+                                for (int q = 0; q < ni; ++q) internal += sw[q];
+                            }
+                            bool fresh = false;
+                            if (valid && hh.inner == 0) {
+                                fresh = !a.in2hop[hh.x];
+                                if (fresh) a.in2hop[hh.x] = 1;
+                                a.triwgt[hh.x] += hh.w;
+                            }
+                            const unsigned fm = __ballot_sync(0xffffffffu, fresh);
+                            if (fresh) cc.twohop[n2 + __popc(fm & lt)] = hh.x;
+                            n2 += __popc(fm);
                             __syncwarp();
-                            const int ni = __popc(im);
-                            for (int q = 0; q < ni; ++q) internal += sw[q];
                         }
-                        // the others are two-hop candidates: distinct x, one lane each
-                        bool fresh = false;
-                        if (ok && !in_nbd) {
-                            fresh = !a.in2hop[x];
-                            if (fresh) a.in2hop[x] = 1;
-                            a.triwgt[x] += wgt;
-                        }
-                        const unsigned fm = __ballot_sync(0xffffffffu, fresh);
-                        if (fresh) twohop[n2 + __popc(fm & lt)] = x;
-                        n2 += __popc(fm);
-                        __syncwarp();  // the next chunk or pair may touch the same x from another lane
                     }
+                } else if (r + 1 < rounds) {
+                    produce((r + 1) * P + wib - 1, set ^ 1);
                 }
+                __syncthreads();
             }
-            int fail = 0;
-            int64_t ntop = 0;         // deletion stack size, built and replayed by the warp
-            int32_t ncl_members = 0;  // size of the cluster just cut out (lane 0)
-            if (lane == 0) {
-                sort_ids(twohop, n2);
-                double potential = 0;
-                for (int64_t k = 0; k < n2; ++k) {
-                    const int32_t x = twohop[k];
-                    cand[k].vertex = x;
-                    cand[k].pad = 0;
-                    cand[k].wgt = a.triwgt[x];
-                    potential += a.triwgt[x];
-                    a.triwgt[x] = 0;
-                    a.in2hop[x] = 0;
-                }
-                introsort(cand, cand + n2, [](const Cand& p, const Cand& q) { return p.wgt > q.wgt; });
-                double ratio = internal / (internal + potential);
-                int64_t maxind = -1;
-                double num = 0, den = 0;
-                for (int64_t k = 0; k < n2; ++k) {
-                    num += cand[k].wgt;
-                    den += a.pv[cand[k].vertex];
-                    const double nr = (internal + num) / (internal + potential + den);
-                    if (nr > ratio) {
-                        ratio = nr;
-                        maxind = k;
-                    }
-                }
-                for (int64_t k = 0; k <= maxind; ++k) {
-                    S.insert(cand[k].vertex - base);
-                    a.clustered[cand[k].vertex] = 1;
-                }
-                // The reference clears the bit of every neighbour of u (Decomposition.h:879-883).
-                // Only the alive ones were set, and a dead neighbour may belong to another
-                // component that a different thread is processing right now, so clear
-                // exactly the bits this seed set.
-                for (int64_t j = r0; j < r1; ++j)
-                    if (a.st[fwd_slot(u, j, a.nb, a.partner)] != ST_N) a.nbd[a.nb[j]] = 0;
-
-                if (out + S.size > vb + nv || ncl >= nv) {  // clusters must partition the component
-                    atomicOr(a.err, (unsigned)DEV_ERR_SCRATCH);
-                    fail = 1;
-                } else {
-                    a.hdr_seed[vb + ncl] = u;
-                    a.hdr_start[vb + ncl] = out;
-                    a.hdr_size[vb + ncl] = S.size;
-                    ncl_members = S.size;
-                    for (int32_t p = S.head; p != -1; p = S.next[p]) a.out_vert[out++] = S.key[p] + base;
-                    ++ncl;
-                }
+            if (wib == 0) {
+                int fail = 0;
+                int32_t nm = 0;
+                if (lane == 0) fail = seed_select(a, cc, u, internal, n2, &nm);
+                __syncwarp();
+                fail = __shfl_sync(0xffffffffu, fail, 0);
+                if (!fail) seed_delete(a, cc, __shfl_sync(0xffffffffu, nm, 0), __shfl_sync(0xffffffffu, cc.out, 0), sw);
+                if (lane == 0) s_fail = fail;
             }
-            __syncwarp();
-            if (__shfl_sync(0xffffffffu, fail, 0)) break;
-            // The deletion stack: every still-'Y' edge of the cluster's members, members
-            // in set-iteration order (the list lane 0 just wrote to out_vert) and each
-            // member's row in order, 32 row entries at a time.  An edge between two
-            // members is pushed from the first member's row only ('S' afterwards).
-            {
-                const int32_t nm = __shfl_sync(0xffffffffu, ncl_members, 0);
-                const int64_t mbase = __shfl_sync(0xffffffffu, out, 0) - nm;
-                int64_t top = 0;
-                bool full = false;
-                for (int32_t q = 0; q < nm && !full; ++q) {
-                    const int32_t z = a.out_vert[mbase + q];
-                    const int64_t j1 = a.off[z + 1];
-                    for (int64_t jb = a.off[z]; jb < j1; jb += 32) {
-                        const int64_t j = jb + lane;
-                        int64_t f = -1;
-                        bool push = false;
-                        if (j < j1) {
-                            f = fwd_slot(z, j, a.nb, a.partner);
-                            push = a.st[f] == ST_Y;
-                        }
-                        const unsigned pm = __ballot_sync(0xffffffffu, push);
-                        const int np = __popc(pm);
-                        if (top + np > cd.scap) {
-                            if (lane == 0) atomicOr(a.err, (unsigned)DEV_ERR_STACK_OVERFLOW);
-                            full = true;  // stop scanning; the cascade still runs on what was pushed
-                            break;
-                        }
-                        if (push) {
-                            dstack[top + __popc(pm & lt)] = DelEntry{(int32_t)f, z, a.nb[j], 0};
-                            a.st[f] = ST_S;
-                        }
-                        top += np;
-                        __syncwarp();
-                    }
-                }
-                ntop = top;
-            }
-            __syncwarp();
-            delete_and_clean_warp(a, dstack, ntop, cd.scap, sw);
+            __syncthreads();
+            if (s_fail) break;
         }
-        if (lane == 0) a.ncl[c] = ncl;
+        if (threadIdx.x == 0) a.ncl[c] = cc.ncl;
     }
 }
 
@@ -658,11 +895,45 @@ __global__ void k_widen(const int32_t* __restrict__ in, int64_t* __restrict__ ou
         out[i] = in[i];
 }
 
+// Components of at least `thr` vertices (the block kernel's) and the largest vertex count among them.
+__global__ void k_big_count(const CompDesc* __restrict__ comps, int64_t nc, int64_t thr, unsigned* __restrict__ nbig,
+                            unsigned long long* __restrict__ maxv)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x)
+        if (comps[c].vcount >= thr) {
+            atomicAdd(nbig, 1u);
+            atomicMax(maxv, (unsigned long long)comps[c].vcount);
+        }
+}
+
 __global__ void k_halve(int64_t* __restrict__ ne, int64_t ncl)
 {
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ncl; g += (int64_t)gridDim.x * blockDim.x)
         ne[g] /= 2;
 }
+
+// The side stream joined back into the main stream (explicitly, or on an early
+// return, before the scratch the side kernel uses is freed).
+struct SideJoin {
+    cudaStream_t side = nullptr, main = nullptr;
+    void join()
+    {
+        if (!side) return;
+        cudaEvent_t done;
+        if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(done, side);
+            cudaStreamWaitEvent(main, done, 0);
+            cudaEventDestroy(done);
+        } else {
+            cudaStreamSynchronize(side);
+        }
+        side = nullptr;
+    }
+    ~SideJoin()
+    {
+        if (side) cudaStreamSynchronize(side);
+    }
+};
 
 }  // namespace
 
@@ -743,7 +1014,7 @@ int extract_clusters(rtr_graph* g)
     k_comp_sizes<<<gc, kBlock, 0, s>>>(comps, nc, n, csorted, B, acount, bneed, sneed);
     exclusive_scan_i64(bneed, boff, nc, d_tot, ltmp, s);
     exclusive_scan_i64(sneed, soff, nc, d_tot + 1, ltmp, s);
-    k_comp_finish<<<gc, kBlock, 0, s>>>(comps, nc, boff, soff, sneed, okeys);
+    k_comp_finish<<<gc, kBlock, 0, s>>>(comps, nc, boff, soff, sneed, okeys, g->extract_big);
     uint64_t* order = radix_sort_u64(okeys, oalt, nc, 64, otmp, s);
     g->launches += 9 + 24;
     int64_t tots[2] = {0, 0};
@@ -795,12 +1066,57 @@ int extract_clusters(rtr_graph* g)
     RTR_CUDA_TRY(cudaMemsetAsync(a.in2hop, 0, n + 16, s));
     RTR_CUDA_TRY(cudaMemsetAsync(a.triwgt, 0, sizeof(double) * (n + 1), s));
     RTR_CUDA_TRY(cudaMemsetAsync(next_comp, 0, sizeof(unsigned) * 2, s));
+    // components of at least extract_big vertices: a thread block each, on the
+    // side stream, while the others take a warp each here
+    unsigned* d_big = (unsigned*)sc.get(sizeof(unsigned) * 2);
+    unsigned long long* d_maxv = (unsigned long long*)sc.get(sizeof(unsigned long long));
+    if (!d_big || !d_maxv) {
+        set_error("device allocation failed (extract split)");
+        return RTR_ERR_CUDA;
+    }
+    RTR_CUDA_TRY(cudaMemsetAsync(d_big, 0, sizeof(unsigned) * 2, s));
+    RTR_CUDA_TRY(cudaMemsetAsync(d_maxv, 0, sizeof(unsigned long long), s));
+    k_big_count<<<gc, kBlock, 0, s>>>(comps, nc, g->extract_big, d_big, d_maxv);
+    unsigned nbig = 0;
+    unsigned long long maxv = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&nbig, d_big, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaMemcpyAsync(&maxv, d_maxv, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    g->launches += 1;
+    SideJoin side_join;  // an early return waits for the side stream before scratch is freed
+    if (nbig > 0) {
+        const int64_t hcap = (int64_t)maxv + 32;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+        const int64_t per_block = hcap * ((int64_t)sizeof(int32_t) + 2 * (kBigWarps - 1) * (int64_t)sizeof(PairHit));
+        int64_t bgrid = std::min<int64_t>((int64_t)nbig, sms);
+        bgrid = std::max<int64_t>(1, std::min<int64_t>(bgrid, (4ll << 30) / per_block));
+        int32_t* fbuf = (int32_t*)sc.get(sizeof(int32_t) * (size_t)(bgrid * hcap));
+        PairHit* hbuf = (PairHit*)sc.get(sizeof(PairHit) * (size_t)(bgrid * 2 * (kBigWarps - 1) * hcap));
+        if (!fbuf || !hbuf) {
+            set_error("device allocation failed (extract pair buffers)");
+            return RTR_ERR_CUDA;
+        }
+        if (!g->side) RTR_CUDA_TRY(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking));
+        cudaEvent_t ready;
+        RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        RTR_CUDA_TRY(cudaEventRecord(ready, s));
+        RTR_CUDA_TRY(cudaStreamWaitEvent(g->side, ready, 0));
+        cudaEventDestroy(ready);
+        side_join.side = g->side;
+        side_join.main = s;
+        k_extract_big<<<(unsigned)bgrid, kBigBlock, 0, g->side>>>(a, comps, order, (int64_t)nbig, next_comp + 1,
+                                                                   fbuf, hbuf, hcap);
+        g->launches += 1;
+    }
     {
         const int blk = kExtractBlock;
-        const int64_t warps = (nc + 0);  // one component per warp
+        const int64_t warps = (int64_t)nc - nbig;  // one component per warp
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((warps + 3) / 4, grid_for(1 << 30, blk, 16)));
         ktime_begin(g, KT_EXTRACT);
-        k_extract_components<<<blocks, blk, 0, s>>>(a, comps, order, nc, next_comp);
+        if (warps > 0)
+            k_extract_components<<<blocks, blk, 0, s>>>(a, comps, order + nbig, warps, next_comp);
+        if (nbig > 0) side_join.join();
         ktime_end(g, KT_EXTRACT);
         g->launches += 1;
     }

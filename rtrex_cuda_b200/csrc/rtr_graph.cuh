@@ -92,6 +92,9 @@ struct rtr_graph {
     // try_wait rounds of a window's first wait (0: the full limit), unit stack entries (-1: as sized)
     int64_t clean_wait_first = 0;
     int64_t clean_stack_limit = -1;
+    // extraction: components of at least this many vertices are replayed by a
+    // whole thread block (the two-hop scan's pairs worked out ahead), the others by a warp
+    int64_t extract_big = 512;
     cudaStream_t side = nullptr;  // second stream of the graph (created on first use)
 
     // stage timings from CUDA events (ms)
