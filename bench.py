@@ -440,7 +440,7 @@ def batched_leg(args, dev):
 REF_CUDA_BIN = os.path.join(ROOT, "oracle", "_ref", "RTRex_CUDA")
 
 
-def gpu_baseline_leg(dev, timeout_s=240):
+def gpu_baseline_leg(dev, timeout_s=120):
     """The reference's CUDA port (RTRex_CUDA, built from its sources for sm_100a
     by oracle/Makefile ref-cuda) on configs 1 and 2: its own phase timers, and how
     its results diverge from the reference's sequential code (its outputs are not

@@ -152,9 +152,10 @@ int rtr_set_extract_split(rtr_graph* g, int64_t min_vertices);
 /* Bounds of the clean's device-side self-checks, to test their error reports
  * (no counterpart in the reference).  first_wait_rounds limits the first
  * bounded wait of the warp-per-unit replay on each window's asynchronous copies
- * (0 = the full limit); when it runs out the warp reports it and drains the
- * copies under the full limit before it stops.  stack_entries caps every unit's
- * cascade-stack region (-1 = sized to the unit).  A check that fires makes
+ * (0 = the full limit; a lowered limit probes the barrier without blocking);
+ * when it runs out the warp reports it and drains the copies under the full
+ * limit before it stops.  stack_entries caps the depth of every unit's cascade
+ * stack (-1 = bounded only by the unit's own region).  A check that fires makes
  * rtr_clean return RTR_ERR_DEVICE with the condition named in rtr_last_error();
  * the graph's results are then incomplete but the device stays usable. */
 int rtr_set_clean_checks(rtr_graph* g, int64_t first_wait_rounds, int64_t stack_entries);
@@ -228,6 +229,30 @@ int rtr_connected_components(rtr_graph* g, int64_t* n_components);
 /* Copy the components: component k has vertices vert[off[k] .. off[k+1]) in
  * discovery order.  Sizes: off[n_components+1], vert[n]. */
 int rtr_get_components(const rtr_graph* g, int64_t* off, int64_t* vert);
+
+/* The nucleus (truss-hierarchy) path of the reference's nucleus driver: the
+ * graph relabelled by (degree, id), every edge's triangles listed, edges
+ * peeled level by level (an edge goes at level c when it is in fewer than c
+ * live triangles; kappa = c-1) in the reference's LIFO order, and the edge
+ * hierarchy turned into clusters, highest level first.  *n_clusters receives
+ * their number.  Results are bit-identical to the reference (its
+ * fixed-size arrays overrun on some inputs, e.g. K20, where its output is
+ * undefined).
+ * Replaces: clustering/nucleus.cpp:12-81 with Escape/Digraph.h:84-134 and
+ *           Escape/Nucleus.h:78-565 (betterWedgeEnumerator, storeAllTriangles, nuclei). */
+int rtr_nucleus(rtr_graph* g, int64_t* n_clusters);
+
+/* The clusters of the last rtr_nucleus, in the order the driver writes them:
+ * cluster k has level c[k], nv[k] vertices, ne[k] edges, parent[k] (-1: none)
+ * and members vert[off[k] .. off[k+1]) in original labels, ascending in the
+ * relabelled order.  Sizes: c/nv/ne/parent[n_clusters], off[n_clusters+1],
+ * vert[n_members]; any pointer may be NULL (call once with NULLs for the sizes). */
+int rtr_get_nuclei(const rtr_graph* g, int64_t* n_clusters, int64_t* n_members, int64_t* c, int64_t* nv,
+                   int64_t* ne, int64_t* parent, int64_t* off, int64_t* vert);
+
+/* Write the clusters of the last rtr_nucleus to `path` exactly as the nucleus
+ * driver writes its output file (nucleus.cpp:62-76). */
+int rtr_write_nuclei(const rtr_graph* g, const char* path);
 
 /* Write <name>-decomposition.txt / -stats.txt / -freq.txt / -cut.txt for the
  * connected components, as RTRex.cpp:203-204 prints them through

@@ -111,6 +111,9 @@ def lib():
     L.rtr_set_clean_split.argtypes = [_vp, _i64, ctypes.c_double]
     L.rtr_set_clean_checks.argtypes = [_vp, _i64, _i64]
     L.rtr_set_extract_split.argtypes = [_vp, _i64]
+    L.rtr_nucleus.argtypes = [_vp, P(_i64)]
+    L.rtr_get_nuclei.argtypes = [_vp, P(_i64), P(_i64)] + [_vp] * 6
+    L.rtr_write_nuclei.argtypes = [_vp, ctypes.c_char_p]
     L.rtr_get_clean_split.argtypes = [_vp, P(_i64), P(ctypes.c_double)]
     L.rtr_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, _i64, ctypes.c_int, P(_vp)]
     L.rtr_server_add_graph.argtypes = [_vp, _vp, _vp, _i64, _i64, ctypes.c_int, P(_i64)]
@@ -360,6 +363,28 @@ class Graph:
         most `max_mean_list` entries on average replay in parallel rounds (one
         thread block each), the others one warp per unit (same bits)."""
         _check(lib().rtr_set_clean_split(self._h, int(min_seeds), float(max_mean_list)))
+
+    def nucleus(self) -> int:
+        """The nucleus (truss-hierarchy) path; returns the number of clusters."""
+        k = _i64()
+        _check(lib().rtr_nucleus(self._h, ctypes.byref(k)))
+        return int(k.value)
+
+    def nuclei(self):
+        """(c, nv, ne, parent, off, vert) of the last nucleus run, in output order."""
+        k, nm = _i64(), _i64()
+        _check(lib().rtr_get_nuclei(self._h, ctypes.byref(k), ctypes.byref(nm), None, None, None, None, None,
+                                    None))
+        c, nv, ne, par = (np.zeros(max(1, k.value), np.int64) for _ in range(4))
+        off = np.zeros(k.value + 1, np.int64)
+        vert = np.zeros(max(1, nm.value), np.int64)
+        _check(lib().rtr_get_nuclei(self._h, ctypes.byref(k), ctypes.byref(nm), _ptr(c), _ptr(nv), _ptr(ne),
+                                    _ptr(par), _ptr(off), _ptr(vert)))
+        kk = k.value
+        return c[:kk], nv[:kk], ne[:kk], par[:kk], off, vert[:nm.value]
+
+    def write_nuclei(self, path: str):
+        _check(lib().rtr_write_nuclei(self._h, path.encode()))
 
     def set_extract_split(self, min_vertices: int = 512):
         """Components of at least min_vertices vertices are extracted by a thread

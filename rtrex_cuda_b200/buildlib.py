@@ -25,7 +25,7 @@ CLI = os.path.join(HERE, "rtrex_b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
            "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["primitives.cu", "graph.cu", "count.cu", "count_rows.cu", "clean.cu", "clean_rounds.cu", "extract.cu", "capi.cu", "io.cpp", "noalloc.cu", "components.cu", "expand.cu", "escape.cu", "serve.cpp", "gen.cu"]
+SOURCES = ["primitives.cu", "graph.cu", "count.cu", "count_rows.cu", "clean.cu", "clean_rounds.cu", "extract.cu", "capi.cu", "io.cpp", "noalloc.cu", "components.cu", "expand.cu", "escape.cu", "serve.cpp", "gen.cu", "nucleus.cu"]
 
 
 def _nvcc() -> str:

@@ -245,6 +245,7 @@ struct CleanArgs {
     double inv_n;
     const StackEntry* seeds;
     long wait_first;  // try_wait rounds of a window's first wait (kWaitLimit unless lowered to test the report)
+    int64_t depth_limit;  // cascade-stack depth that counts as an overflow (-1: only the unit's region bounds it)
 };
 
 constexpr int kCleanBlock = 128;
@@ -285,6 +286,19 @@ __device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigne
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+
+// Non-blocking probe of the barrier phase (try_wait may suspend the thread for a
+// while before it answers; test_wait answers at once).
+__device__ __forceinline__ bool mbar_ready(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
 }
 
 __device__ __forceinline__ bool mbar_done(uint64_t* bar, unsigned parity)
@@ -381,6 +395,10 @@ __device__ __forceinline__ bool apply_group(const CleanArgs& a, const Group& g, 
     }
     const int np = __popc(b1) + __popc(b2);
     if (np) {
+        if (a.depth_limit >= 0 && ws.gtop + ws.scount + np > a.depth_limit) {  // a lowered bound (tests)
+            if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_STACK_OVERFLOW);
+            return false;
+        }
         if (ws.scount + np > kSmemStack) {  // spill the shared part, oldest first
             if (ws.gtop + ws.scount > ws.cap) {
                 if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_STACK_OVERFLOW);
@@ -604,7 +622,12 @@ __global__ void __launch_bounds__(kCleanBlock)
                         __syncwarp();
                         if (bytes) bulk_to_smem(&sm.went[lane][0], a.tl + wseed.t0, bytes, &sm.bar);
                         long it = 0;
-                        while (!mbar_done(&sm.bar, bar_phase) && ++it < a.wait_first) {
+                        if (a.wait_first < kWaitLimit) {  // a lowered bound (tests): probe without waiting
+                            while (!mbar_ready(&sm.bar, bar_phase) && ++it < a.wait_first) {
+                            }
+                        } else {
+                            while (!mbar_done(&sm.bar, bar_phase) && ++it < a.wait_first) {
+                            }
                         }
                         if (it >= a.wait_first) {  // report, give the copies one more bounded wait, stop
                             if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_WAIT);
@@ -768,7 +791,7 @@ int initial_clean(rtr_graph* g, double eps)
         }
         if ((int64_t)nbig < (int64_t)nu) {
             CleanArgs ca{g->tl, rec, g->pv, 1 / (double)n, seeds,
-                         g->clean_wait_first > 0 ? (long)g->clean_wait_first : kWaitLimit};
+                         g->clean_wait_first > 0 ? (long)g->clean_wait_first : kWaitLimit, g->clean_stack_limit};
             // one warp per unit, persistent over the unit list (largest units first)
             const int64_t nsmall = (int64_t)nu - (int64_t)nbig;
             int blocks = (int)std::min<int64_t>((nsmall + kCleanWarps - 1) / kCleanWarps,

@@ -1,6 +1,7 @@
 // rtrex_b200: drop-in command line for the decomposition path.
 //
 //   rtrex_b200 <graph_file> <output_name> <eps> [gpu_device] [--prefix P] [--simplify] [--expand T]
+//   rtrex_b200 --nucleus <graph_file> <output_file>
 //
 // Same positional arguments and outputs as RTRex_CUDA (RTRex_CUDA/main.cu:343-391):
 // writes <P><output_name>-{decomposition,stats,freq,cut}.txt with P defaulting
@@ -18,8 +19,34 @@
 #include <cstring>
 #include <string>
 
+// rtrex_b200 --nucleus <graph_file> <output_file>: the reference's nucleus
+// driver (RTRex_Sequential/clustering/nucleus.cpp:12-81) -- the truss hierarchy
+// written to <output_file> in its format.
+static int run_nucleus(const char* graph, const char* out)
+{
+    rtr_graph* g = nullptr;
+    int rc = rtr_graph_create_from_escape_file(graph, 0, 0, &g);
+    if (rc) return rc;
+    printf("Loaded graph\n");
+    int64_t k = 0;
+    if (!(rc = rtr_nucleus(g, &k))) {
+        printf("Compute nuclei\n%lld clusters\n", (long long)k);
+        rc = rtr_write_nuclei(g, out);
+    }
+    rtr_graph_destroy(g);
+    return rc;
+}
+
 int main(int argc, char** argv)
 {
+    if (argc == 4 && !strcmp(argv[1], "--nucleus")) {
+        const int rc = run_nucleus(argv[2], argv[3]);
+        if (rc != RTR_OK) {
+            fprintf(stderr, "Error: %s\n", rtr_last_error());
+            return 1;
+        }
+        return 0;
+    }
     std::string prefix = "RTRex-CUDA-";
     int flags = 0;
     long long threshold = 0;

@@ -61,6 +61,11 @@ struct rtr_graph {
     int32_t* x_scv = nullptr;     // moved vertices, ascending
     double* x_scx = nullptr;      // their scores
 
+    // nucleus (truss-hierarchy) clusters in output order, members in original labels
+    bool nuc_done = false;
+    std::vector<int64_t> nuc_c, nuc_nv, nuc_ne, nuc_parent, nuc_off, nuc_vert;
+    float ms_nucleus = 0;
+
     // connected components of the original graph, creation order, BFS discovery order inside
     int64_t ncc = 0;
     int64_t* cc_off = nullptr;   // [ncc+1]
