@@ -71,7 +71,7 @@ def parse_args():
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--rmat-scale", type=int, default=24)
     ap.add_argument("--count-mode", type=int, default=0, help="rtr_set_count_mode for --workload rmat_count")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batch", "serve", "rmat_count"],
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batch", "serve", "rmat_count", "bundled"],
                     help="batch: the 4,096-graph SBM batch, batched vs per-graph plain decompositions")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     return ap.parse_args()
@@ -396,6 +396,51 @@ def rmat_count_arm(args):
             "triangles": r["triangles"], "triangles_per_s": r["triangles_per_s"], "e2e": r.get("e2e"),
             "roofline": r["roofline_count"], "gpu_launches": r["gpu_launches_per_count"] * r["steps"],
             "kernel_ms": r["kernel_ms"], "generation_and_csr_build_ms": r["generation_and_csr_build_ms"]}
+    print(json.dumps(line), flush=True)
+
+
+def bundled_arm(args):
+    """--workload bundled: the reference's own bundled graphs (clean_email,
+    clean_astro, random_graph_rtr; committed copies under tests/golden/data/)
+    decomposed at eps, device stage times (CUDA events, mean of --steps after
+    --warmup) beside the reference's phase timers (oracle/_ref/RTRex, mode s,
+    one core) on the same box."""
+    import torch
+    import rtrex_cuda_b200 as rtr
+    from rtrex_cuda_b200 import graphgen
+    torch.cuda.set_device(0)
+    out = {}
+    for name in ("clean_email", "clean_astro", "random_graph_rtr"):
+        path = os.path.join(ROOT, "tests", "golden", "data", name + ".txt.gz")
+        n, u, v = graphgen.read_escape(path)
+        ms = {"count": [], "clean": [], "extract": [], "decompose": []}
+        with rtr.Graph.from_edges(n, u, v) as g:
+            for k in range(args.warmup + args.steps):
+                ncl = g.decompose(args.eps)
+                st, km = g.stats(), g.kernel_ms()
+                if k >= args.warmup:
+                    ms["count"].append(st["ms_count"])
+                    ms["clean"].append(st["ms_clean"])
+                    ms["extract"].append(st["ms_extract"])
+                    ms["decompose"].append(km["decompose"])
+        res = {"n": n, "m": int(u.size), "clusters": ncl,
+               "device_ms": {k: float(np.mean(x)) for k, x in ms.items()}}
+        if os.path.exists(REF_BIN):
+            with tempfile.TemporaryDirectory() as td:
+                p2 = os.path.join(td, "g.txt")
+                graphgen.write_escape(p2, n, u, v)
+                r = subprocess.run([REF_BIN, p2, "bench", repr(args.eps), "s"], cwd=td, capture_output=True,
+                                   text=True, timeout=900, env=dict(os.environ, OMP_NUM_THREADS="1"))
+            grab = lambda k: float(re.search(re.escape(k) + r":\s*([0-9.eE+-]+)s", r.stdout).group(1)) * 1e3
+            res["reference_ms_1core"] = {"count": grab("Time for getting the weights"),
+                                         "clean": grab("Time for the initial clean"),
+                                         "extract": grab("Time for getting the clusters")}
+        out[name] = res
+    line = {"metric": "decomposed edges/s (count+clean+extract)", "unit": "edges/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+            "data": "the reference's bundled graphs", "config": {"workload": "bundled", "eps": args.eps},
+            "value": sum(r["m"] for r in out.values()) / sum(r["device_ms"]["decompose"] / 1e3 for r in out.values()),
+            "graphs": out}
     print(json.dumps(line), flush=True)
 
 
@@ -814,6 +859,13 @@ def main():
         import torch.distributed as dist
         if dist.is_available() and dist.is_initialized():
             dist.destroy_process_group()
+        return
+    if args.workload == "bundled":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the bundled workload reports the reference's "
+                              "phase timers beside the device times in its own line"}), flush=True)
+            return
+        bundled_arm(args)
         return
     if args.workload == "rmat_count":
         if args.impl == "reference":
