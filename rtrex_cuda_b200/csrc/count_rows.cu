@@ -59,7 +59,50 @@ struct RowsArgs {
     int heavy_edge;  // deg x + deg y from which perEdge is folded here (k_edge_fold left it)
     int light;       // vertices below this degree: a thread
     int hub;         // vertices from this degree: a thread block
+    // every kIdxStride-th neighbour of each hub (hub_pos[v]: v's place in the hub
+    // list, -1 for the others), so that a lookup in a hub's long row searches
+    // this compact array and then a single window of the row
+    const int32_t* hub_pos;
+    const int64_t* idx_off;
+    const int32_t* idx;
 };
+
+constexpr int kIdxStride = 32;
+
+// Lower bound of v in the row of y (the range [lo, hi) of the caller is y's
+// whole row): through y's sample index when y is a hub.  A search that the
+// index places before lo returns that position; the callers only count hits at
+// or after lo.
+__device__ __forceinline__ int64_t row_lower_bound(const RowsArgs& a, int32_t y, int64_t lo, int64_t hi, int32_t v)
+{
+    const int32_t h = a.hub_pos ? a.hub_pos[y] : -1;
+    if (h < 0) return lower_bound_row(a.nb, lo, hi, v);
+    const int64_t s0 = a.idx_off[h], s1 = a.idx_off[h + 1];
+    int64_t l = s0, r = s1;  // first sample above v
+    while (l < r) {
+        const int64_t mid = (l + r) >> 1;
+        if (a.idx[mid] <= v) l = mid + 1;
+        else r = mid;
+    }
+    const int64_t base = a.off[y], end = a.off[y + 1];
+    if (l == s0) return base;
+    const int64_t w0 = base + (l - 1 - s0) * kIdxStride;
+    const int64_t w1 = w0 + kIdxStride < end ? w0 + kIdxStride : end;
+    return lower_bound_row(a.nb, w0, w1, v);
+}
+
+// Common neighbours of the short ascending range [s0, s1) and hub y's row, in
+// ascending order: f(z).  One thread.
+template <typename F>
+__device__ __forceinline__ void intersect_with_hub(const RowsArgs& a, int64_t s0, int64_t s1, int32_t y, F&& f)
+{
+    const int64_t b0 = a.off[y], b1 = a.off[y + 1];
+    for (int64_t p = s0; p < s1; ++p) {
+        const int32_t x = a.nb[p];
+        const int64_t pos = row_lower_bound(a, y, b0, b1, x);
+        if (pos < b1 && a.nb[pos] == x) f(x);
+    }
+}
 
 __device__ __forceinline__ bool owns_heavy(const RowsArgs& a, int32_t x, int32_t y, int dx, int dy)
 {
@@ -80,17 +123,21 @@ __global__ void __launch_bounds__(kLightBlock) k_rows_light(RowsArgs a)
             const int dy = a.deg[y];
             const int64_t dxy = (int64_t)dx * (int64_t)dy;
             const int64_t b0 = a.off[y], b1 = a.off[y + 1];
+            const bool y_hub = a.hub_pos && a.hub_pos[y] >= 0;  // x is light: its row is the short one
             if (owns_heavy(a, x, y, dx, dy)) {
                 double peacc = 0.0;
-                intersect_rows(a.nb, a0, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) {
+                auto f = [&](int32_t z) {
                     const double w = 1.0 / (double)(dxy * (int64_t)a.deg[z]);
                     peacc += w;
                     if (z > y) pvacc += w;
-                });
+                };
+                if (y_hub) intersect_with_hub(a, a0, a1, y, f);
+                else intersect_rows(a.nb, a0, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) { f(z); });
                 a.pe[i] = peacc;
             } else {
-                intersect_rows(a.nb, i + 1, a1, b0, b1, a.gallop,
-                               [&](int32_t z, int64_t, int64_t) { pvacc += 1.0 / (double)(dxy * (int64_t)a.deg[z]); });
+                auto f = [&](int32_t z) { pvacc += 1.0 / (double)(dxy * (int64_t)a.deg[z]); };
+                if (y_hub) intersect_with_hub(a, i + 1, a1, y, f);
+                else intersect_rows(a.nb, i + 1, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) { f(z); });
             }
         }
         a.pv[x] = pvacc;
@@ -124,7 +171,9 @@ __global__ void __launch_bounds__(kMediumBlock) k_rows_medium(RowsArgs a)
                 const int below = owner ? __popc(__ballot_sync(0xffffffffu, hit && z < y)) : 0;
                 fold_hits(hit, w, s_w[wib], lane, owner ? &peacc : nullptr, &pvacc, below);
             };
-            if (A1 - A0 <= B1 - B0) warp_chunks(a.nb, A0, A1, B0, B1, lane, search, chunk);
+            // A shorter: y's whole row is searched (through its index when y is a hub)
+            auto search_y = [&](int64_t lo, int64_t hi, int32_t v) { return row_lower_bound(a, y, lo, hi, v); };
+            if (A1 - A0 <= B1 - B0) warp_chunks(a.nb, A0, A1, B0, B1, lane, search_y, chunk);
             else warp_chunks(a.nb, B0, B1, A0, A1, lane, search, chunk);
             if (owner && lane == 0) a.pe[i] = peacc;
         }
@@ -169,7 +218,6 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
             const int64_t w1 = w0 + stride < a1 ? w0 + stride : a1;
             return lower_bound_row(a.nb, w0, w1, v);
         };
-        auto search_g = [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(a.nb, lo, hi, v); };
         // producer warp w (1..P) on slot i: y's z > y weights into region(set, w-1)
         auto produce = [&](int64_t i, int set) {
             int64_t len = 0;
@@ -198,7 +246,8 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
                     if (!owner) B0 = lower_bound_row(a.nb, B0, B1, y + 1);  // A holds only z > y
                     warp_chunks(a.nb, B0, B1, A0, A1, lane, search_x, chunk);
                 } else {
-                    warp_chunks(a.nb, A0, A1, B0, B1, lane, search_g, chunk);
+                    auto search_y = [&](int64_t lo, int64_t hi, int32_t v) { return row_lower_bound(a, y, lo, hi, v); };
+                    warp_chunks(a.nb, A0, A1, B0, B1, lane, search_y, chunk);
                 }
                 if (owner && lane == 0) a.pe[i] = peacc;
             }
@@ -245,6 +294,33 @@ __global__ void k_hub_keys(const int32_t* __restrict__ deg, int64_t n, int hub, 
             keys[atomicAdd(nh, 1u)] = ((uint64_t)(0x7fffffff - deg[v]) << 32) | (uint64_t)v;
 }
 
+__global__ void k_hub_index_sizes(const int32_t* __restrict__ hubs, int64_t nh, const int32_t* __restrict__ deg,
+                                  int32_t* __restrict__ hub_pos, int64_t* __restrict__ cnt)
+{
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h <= nh; h += (int64_t)gridDim.x * blockDim.x) {
+        if (h == nh) {
+            cnt[h] = 0;
+            continue;
+        }
+        hub_pos[hubs[h]] = (int32_t)h;
+        cnt[h] = (deg[hubs[h]] + kIdxStride - 1) / kIdxStride;
+    }
+}
+
+// A warp per hub (dealt modulo the warp count): sample k of hub h is its row's entry kIdxStride*k.
+__global__ void k_hub_index_fill(const int32_t* __restrict__ hubs, int64_t nh, const int64_t* __restrict__ off,
+                                 const int32_t* __restrict__ nb, const int64_t* __restrict__ ioff,
+                                 int32_t* __restrict__ idx)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x / 32);
+    for (int64_t h = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; h < nh; h += nwarps) {
+        const int64_t x = hubs[h], base = off[x];
+        const int64_t cnt = ioff[h + 1] - ioff[h];
+        for (int64_t k = lane; k < cnt; k += 32) idx[ioff[h] + k] = nb[base + k * kIdxStride];
+    }
+}
+
 __global__ void k_hub_ids(const uint64_t* __restrict__ keys, int64_t nh, int32_t* __restrict__ ids)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nh; i += (int64_t)gridDim.x * blockDim.x)
@@ -260,7 +336,7 @@ int count_rows(rtr_graph* g, Scratch& sc)
     cudaStream_t s = g->stream;
     const int64_t n = g->n;
     RowsArgs a{g->offsets, g->nbors, g->deg, n, g->pe, g->pv, g->tune_gallop, g->tune_edge, g->tune_heavy,
-               g->count_hub};
+               g->count_hub, nullptr, nullptr, nullptr};
     if (a.hub < a.light) a.hub = a.light;
     uint64_t* keys = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
     uint64_t* alt = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
@@ -303,6 +379,32 @@ int count_rows(rtr_graph* g, Scratch& sc)
             return RTR_ERR_CUDA;
         }
         cap += 32;
+        // the hubs' sample index
+        int32_t* hub_pos = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+        int64_t* icnt = (int64_t*)sc.get(sizeof(int64_t) * (nh + 1));
+        int64_t* ioff = (int64_t*)sc.get(sizeof(int64_t) * (nh + 1));
+        int64_t* itmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(nh + 1));
+        int64_t* itot = (int64_t*)sc.get(sizeof(int64_t) * 2);
+        if (!hub_pos || !icnt || !ioff || !itmp || !itot) {
+            set_error("device allocation failed (hub index)");
+            return RTR_ERR_CUDA;
+        }
+        RTR_CUDA_TRY(cudaMemsetAsync(hub_pos, 0xff, sizeof(int32_t) * (n + 1), s));
+        k_hub_index_sizes<<<grid_for(nh, 256), 256, 0, s>>>(hubs, nh, g->deg, hub_pos, icnt);
+        exclusive_scan_i64(icnt, ioff, nh + 1, itot, itmp, s);
+        int64_t ntot = 0;
+        RTR_CUDA_TRY(cudaMemcpyAsync(&ntot, itot, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        RTR_CUDA_TRY(cudaStreamSynchronize(s));
+        int32_t* idx = (int32_t*)sc.get(sizeof(int32_t) * (ntot + 1));
+        if (!idx) {
+            set_error("device allocation failed (hub index)");
+            return RTR_ERR_CUDA;
+        }
+        k_hub_index_fill<<<grid_for(1ll << 40, 256, 8), 256, 0, s>>>(hubs, nh, g->offsets, g->nbors, ioff, idx);
+        g->launches += 5;
+        a.hub_pos = hub_pos;
+        a.idx_off = ioff;
+        a.idx = idx;
     }
     cudaEvent_t ready = nullptr, joined = nullptr;
     if (hub_grid > 0) {
