@@ -23,8 +23,10 @@ def _fresh_decomposition_still_exact():
     n, u, v = helpers.case_graph(name)
     (_, _, _), c, s0, s1, cl, s2 = helpers.oracle_run(name, eps)
     with rtr.Graph.from_edges(n, u, v) as g:
-        assert g.decompose(eps) == len(cl)
+        assert g.count() == s0.total
+        assert g.clean(eps) == s1.total
         assert (g.status() == s1.status).all()
+        assert g.extract() == len(cl)
         got = g.clusters()
         assert (got.vert == cl.vert).all() and (got.off == cl.off).all()
 
