@@ -28,6 +28,7 @@
 // autotuner (rtr_autotune) times candidates on the graph itself.
 #include "intersect.cuh"
 #include "primitives.cuh"
+#include "rowsets.cuh"
 #include "rtr_graph.cuh"
 
 namespace rtr {
@@ -117,7 +118,7 @@ constexpr int kHeavyEdgeBlock = 128;
 __global__ void __launch_bounds__(kHeavyEdgeBlock)
     k_edge_count_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                        const int32_t* __restrict__ fwd, const int32_t* __restrict__ heavy_list,
-                       const unsigned* __restrict__ nheavy, int gallop, uint32_t* __restrict__ sup,
+                       const unsigned* __restrict__ nheavy, int gallop, RowSets rs, uint32_t* __restrict__ sup,
                        int64_t* __restrict__ cnt, unsigned long long* __restrict__ total)
 {
     const int lane = threadIdx.x & 31;
@@ -127,11 +128,24 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
     for (int64_t h = (int64_t)blockIdx.x * (kHeavyEdgeBlock / 32) + (threadIdx.x >> 5); h < nh; h += nwarps) {
         const int64_t i = fwd[heavy_list[h]];
         const int32_t u = esrc[i], v = nb[i];
+        const int64_t u0 = off[u], u1 = off[u + 1], v0 = off[v], v1 = off[v + 1];
         unsigned c = 0, above = 0;
-        warp_intersect_part(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, lane, [&](int32_t z, int64_t, int64_t) {
-            ++c;
-            above += (z > v) ? 1u : 0u;
-        });
+        // the shorter row walked against the longer one's hash set, when it has one
+        const bool u_short = u1 - u0 <= v1 - v0;
+        const int32_t t = rs_table(rs, u_short ? v : u);
+        if (t >= 0) {
+            const int32_t zmax = u_short ? nb[v1 - 1] : nb[u1 - 1];
+            warp_scan(nb, u_short ? u0 : v0, u_short ? u1 : v1, zmax, lane,
+                      [&](int32_t z) { return rs_member(rs, t, z); }, [&](bool hit, int32_t z) {
+                          c += hit ? 1u : 0u;
+                          above += (hit && z > v) ? 1u : 0u;
+                      });
+        } else {
+            warp_intersect_part(nb, u0, u1, v0, v1, gallop, lane, [&](int32_t z, int64_t, int64_t) {
+                ++c;
+                above += (z > v) ? 1u : 0u;
+            });
+        }
         c = __reduce_add_sync(0xffffffffu, c);
         above = __reduce_add_sync(0xffffffffu, above);
         if (lane == 0) {
@@ -345,10 +359,17 @@ int count_triangles(rtr_graph* g)
     const int gh = grid_for(1ll << 40, kHeavyEdgeBlock, 16);
     RTR_CUDA_TRY(cudaMemsetAsync(nheavy, 0, sizeof(unsigned), s));
     ktime_begin(g, KT_EDGE_FOLD);
+    // Hash sets of the long rows, for the heavy-edge count and the rows layout:
+    // built when the rows layout is asked for, or may be chosen (2m >= 2^25).
+    RowSets rs{nullptr, nullptr, nullptr, nullptr};
+    if (g->count_mode == 2 || (g->count_mode == 0 && m2 >= (1ll << 25))) {
+        const int rc = build_row_sets(g, sc, kSetDegree, &rs);
+        if (rc) return rc;
+    }
     k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, m, g->pe, g->sup, cnt, g->ctr,
                                       g->tune_gallop, g->tune_edge, heavy_list, nheavy);
     k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->fwd, heavy_list, nheavy,
-                                                      g->tune_gallop, g->sup, cnt, g->ctr);
+                                                      g->tune_gallop, rs, g->sup, cnt, g->ctr);
     ktime_end(g, KT_EDGE_FOLD);
     exclusive_scan_i64(cnt, g->tl_off, m2 + 1, nullptr, tmp, s);
     g->launches += 6;
@@ -372,7 +393,7 @@ int count_triangles(rtr_graph* g)
         ktime_begin(g, KT_TRI_FILL);
         ktime_end(g, KT_TRI_FILL);
         ktime_begin(g, KT_VERTEX_FOLD);
-        const int rc = count_rows(g, sc);
+        const int rc = count_rows(g, sc, rs);
         ktime_end(g, KT_VERTEX_FOLD);
         if (rc) return rc;
         RTR_CUDA_TRY(cudaGetLastError());

@@ -15,27 +15,28 @@
 //                  ascending, computed by x's pass from the same intersection.
 // For y > x owning a heavy edge the pass intersects the full rows (perEdge
 // needs every z; the z > y suffix continues perVertex[x]); otherwise it
-// intersects N(x) beyond y with N(y).
+// intersects N(x) beyond y with N(y).  Every intersection walks the shorter
+// range in ascending order and looks its elements up in the longer row: in that
+// row's hash set when it has one (rowsets.cuh; build_row_sets below makes one
+// for every row of at least kSetDegree entries), else by binary search.
 //
 // Three kernels by the degree of x:
-//   k_rows_light   a thread per vertex of degree < light (merge / gallop)
+//   k_rows_light   a thread per vertex of degree < light
 //   k_rows_medium  a warp per vertex of degree in [light, hub): for each y in
-//                  turn the warp walks the shorter row 32 elements at a time,
-//                  every lane binary-searching its element in the longer one,
+//                  turn the warp walks the shorter range 32 elements at a time
 //                  and folds the hits in lane order (ascending z)
 //   k_rows_hub     a thread block per vertex of degree >= hub, hubs in
-//                  descending degree: 7 producer warps take 7 consecutive y at
-//                  once, searching x's row through a shared-memory sample of it
-//                  (every stride-th element) and a one-window global search;
-//                  each writes its y's z > y weights, in order, to its own
-//                  buffer, which warp 0 folds in y order while the producers
-//                  work on the next 7 (double-buffered) -- only the perVertex
-//                  chain itself is sequential.
+//                  descending degree, two blocks per SM: 7 producer warps take
+//                  7 consecutive y at once, each writing its y's z > y weights,
+//                  in order, to its own buffer, which warp 0 folds in y order
+//                  while the producers work on the next 7 (double-buffered) --
+//                  only the perVertex chain itself is sequential.
 // The hub kernel runs on the graph's second stream, concurrently with the
 // other two (it holds the longest dependent chain: ~10^8 adds for the largest
 // R-MAT scale-24 hub).
 #include "intersect.cuh"
 #include "primitives.cuh"
+#include "rowsets.cuh"
 #include "rtr_graph.cuh"
 
 namespace rtr {
@@ -46,7 +47,6 @@ constexpr int kLightBlock = 256;
 constexpr int kMediumBlock = 128;
 constexpr int kHubWarps = 8;
 constexpr int kHubBlock = 32 * kHubWarps;
-constexpr int kHubIndexMax = 11264;  // sample entries of a hub row in shared memory (44 KB, static limit 48 KB)
 
 struct RowsArgs {
     const int64_t* off;
@@ -59,54 +59,31 @@ struct RowsArgs {
     int heavy_edge;  // deg x + deg y from which perEdge is folded here (k_edge_fold left it)
     int light;       // vertices below this degree: a thread
     int hub;         // vertices from this degree: a thread block
-    // every kIdxStride-th neighbour of each hub (hub_pos[v]: v's place in the hub
-    // list, -1 for the others), so that a lookup in a hub's long row searches
-    // this compact array and then a single window of the row
-    const int32_t* hub_pos;
-    const int64_t* idx_off;
-    const int32_t* idx;
+    RowSets rs;
 };
-
-constexpr int kIdxStride = 32;
-
-// Lower bound of v in the row of y (the range [lo, hi) of the caller is y's
-// whole row): through y's sample index when y is a hub.  A search that the
-// index places before lo returns that position; the callers only count hits at
-// or after lo.
-__device__ __forceinline__ int64_t row_lower_bound(const RowsArgs& a, int32_t y, int64_t lo, int64_t hi, int32_t v)
-{
-    const int32_t h = a.hub_pos ? a.hub_pos[y] : -1;
-    if (h < 0) return lower_bound_row(a.nb, lo, hi, v);
-    const int64_t s0 = a.idx_off[h], s1 = a.idx_off[h + 1];
-    int64_t l = s0, r = s1;  // first sample above v
-    while (l < r) {
-        const int64_t mid = (l + r) >> 1;
-        if (a.idx[mid] <= v) l = mid + 1;
-        else r = mid;
-    }
-    const int64_t base = a.off[y], end = a.off[y + 1];
-    if (l == s0) return base;
-    const int64_t w0 = base + (l - 1 - s0) * kIdxStride;
-    const int64_t w1 = w0 + kIdxStride < end ? w0 + kIdxStride : end;
-    return lower_bound_row(a.nb, w0, w1, v);
-}
-
-// Common neighbours of the short ascending range [s0, s1) and hub y's row, in
-// ascending order: f(z).  One thread.
-template <typename F>
-__device__ __forceinline__ void intersect_with_hub(const RowsArgs& a, int64_t s0, int64_t s1, int32_t y, F&& f)
-{
-    const int64_t b0 = a.off[y], b1 = a.off[y + 1];
-    for (int64_t p = s0; p < s1; ++p) {
-        const int32_t x = a.nb[p];
-        const int64_t pos = row_lower_bound(a, y, b0, b1, x);
-        if (pos < b1 && a.nb[pos] == x) f(x);
-    }
-}
 
 __device__ __forceinline__ bool owns_heavy(const RowsArgs& a, int32_t x, int32_t y, int dx, int dy)
 {
     return x < y && dx + dy >= a.heavy_edge;
+}
+
+// The warp's hits of the ascending range S = [s0, s1) in the range [l0, l1) of
+// row w: chunk(hit, z) per 32 elements of S, hits ascending.  Through w's hash
+// set when it has one -- exact because every caller passes either w's whole
+// row, or x's row cut just after y together with an S whose elements all
+// exceed y -- else by binary search.
+template <typename F>
+__device__ __forceinline__ void warp_hits(const RowsArgs& a, int64_t s0, int64_t s1, int32_t w, int64_t l0,
+                                          int64_t l1, int lane, F&& chunk)
+{
+    const int32_t t = rs_table(a.rs, w);
+    if (t >= 0) {
+        const int32_t zmax = a.nb[a.off[w + 1] - 1];
+        warp_scan(a.nb, s0, s1, zmax, lane, [&](int32_t z) { return rs_member(a.rs, t, z); }, chunk);
+    } else {
+        warp_chunks(a.nb, s0, s1, l0, l1, lane,
+                    [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(a.nb, lo, hi, v); }, chunk);
+    }
 }
 
 __global__ void __launch_bounds__(kLightBlock) k_rows_light(RowsArgs a)
@@ -123,21 +100,28 @@ __global__ void __launch_bounds__(kLightBlock) k_rows_light(RowsArgs a)
             const int dy = a.deg[y];
             const int64_t dxy = (int64_t)dx * (int64_t)dy;
             const int64_t b0 = a.off[y], b1 = a.off[y + 1];
-            const bool y_hub = a.hub_pos && a.hub_pos[y] >= 0;  // x is light: its row is the short one
+            const int32_t ty = rs_table(a.rs, y);  // x is light: its row is the one walked
+            // common neighbours of x's range [s0, a1) and y's row, ascending: f(z)
+            auto each = [&](int64_t s0, auto&& f) {
+                if (ty >= 0) {
+                    for (int64_t p = s0; p < a1; ++p) {
+                        const int32_t z = a.nb[p];
+                        if (rs_member(a.rs, ty, z)) f(z);
+                    }
+                } else {
+                    intersect_rows(a.nb, s0, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) { f(z); });
+                }
+            };
             if (owns_heavy(a, x, y, dx, dy)) {
                 double peacc = 0.0;
-                auto f = [&](int32_t z) {
+                each(a0, [&](int32_t z) {
                     const double w = 1.0 / (double)(dxy * (int64_t)a.deg[z]);
                     peacc += w;
                     if (z > y) pvacc += w;
-                };
-                if (y_hub) intersect_with_hub(a, a0, a1, y, f);
-                else intersect_rows(a.nb, a0, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) { f(z); });
+                });
                 a.pe[i] = peacc;
             } else {
-                auto f = [&](int32_t z) { pvacc += 1.0 / (double)(dxy * (int64_t)a.deg[z]); };
-                if (y_hub) intersect_with_hub(a, i + 1, a1, y, f);
-                else intersect_rows(a.nb, i + 1, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) { f(z); });
+                each(i + 1, [&](int32_t z) { pvacc += 1.0 / (double)(dxy * (int64_t)a.deg[z]); });
             }
         }
         a.pv[x] = pvacc;
@@ -149,7 +133,6 @@ __global__ void __launch_bounds__(kMediumBlock) k_rows_medium(RowsArgs a)
     __shared__ double s_w[kMediumBlock / 32][32];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t nwarps = (int64_t)gridDim.x * (kMediumBlock / 32);
-    auto search = [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(a.nb, lo, hi, v); };
     for (int64_t xi = (int64_t)blockIdx.x * (kMediumBlock / 32) + wib; xi < a.n; xi += nwarps) {
         const int32_t x = (int32_t)xi;
         const int dx = a.deg[x];
@@ -171,10 +154,8 @@ __global__ void __launch_bounds__(kMediumBlock) k_rows_medium(RowsArgs a)
                 const int below = owner ? __popc(__ballot_sync(0xffffffffu, hit && z < y)) : 0;
                 fold_hits(hit, w, s_w[wib], lane, owner ? &peacc : nullptr, &pvacc, below);
             };
-            // A shorter: y's whole row is searched (through its index when y is a hub)
-            auto search_y = [&](int64_t lo, int64_t hi, int32_t v) { return row_lower_bound(a, y, lo, hi, v); };
-            if (A1 - A0 <= B1 - B0) warp_chunks(a.nb, A0, A1, B0, B1, lane, search_y, chunk);
-            else warp_chunks(a.nb, B0, B1, A0, A1, lane, search, chunk);
+            if (A1 - A0 <= B1 - B0) warp_hits(a, A0, A1, y, B0, B1, lane, chunk);
+            else warp_hits(a, B0, B1, x, A0, A1, lane, chunk);
             if (owner && lane == 0) a.pe[i] = peacc;
         }
         if (lane == 0) a.pv[x] = pvacc;
@@ -187,11 +168,10 @@ __global__ void __launch_bounds__(kMediumBlock) k_rows_medium(RowsArgs a)
 // of buffer set r&1 (buf holds 2 x (kHubWarps-1) regions of cap doubles per
 // block; cap >= the largest hub degree bounds the hits of one y), while warp 0
 // folds round r-1 from the other set.  One block barrier per round.
-__global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_t* __restrict__ hubs, int64_t nhub,
-                                                         double* __restrict__ buf, int64_t cap)
+__global__ void __launch_bounds__(kHubBlock, 2) k_rows_hub(RowsArgs a, const int32_t* __restrict__ hubs,
+                                                            int64_t nhub, double* __restrict__ buf, int64_t cap)
 {
     constexpr int P = kHubWarps - 1;  // producer warps
-    __shared__ int32_t s_idx[kHubIndexMax];
     __shared__ double s_w[kHubWarps][32];
     __shared__ int64_t s_len[2][P];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -200,24 +180,6 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
         const int32_t x = hubs[h];
         const int dx = a.deg[x];
         const int64_t a0 = a.off[x], a1 = a.off[x + 1], d = a1 - a0;
-        int64_t stride = (d + kHubIndexMax - 1) / kHubIndexMax;
-        if (stride < 32) stride = 32;
-        const int K = (int)((d + stride - 1) / stride);
-        for (int k = threadIdx.x; k < K; k += kHubBlock) s_idx[k] = a.nb[a0 + (int64_t)k * stride];
-        __syncthreads();
-        // lower bound of v in x's whole row: the sample narrows it to one window
-        auto search_x = [&](int64_t, int64_t, int32_t v) -> int64_t {
-            int lo = 0, hi = K;  // first sample above v
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (s_idx[mid] <= v) lo = mid + 1;
-                else hi = mid;
-            }
-            if (lo == 0) return a0;
-            const int64_t w0 = a0 + (int64_t)(lo - 1) * stride;
-            const int64_t w1 = w0 + stride < a1 ? w0 + stride : a1;
-            return lower_bound_row(a.nb, w0, w1, v);
-        };
         // producer warp w (1..P) on slot i: y's z > y weights into region(set, w-1)
         auto produce = [&](int64_t i, int set) {
             int64_t len = 0;
@@ -244,10 +206,9 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
                 };
                 if (B1 - B0 <= A1 - A0) {
                     if (!owner) B0 = lower_bound_row(a.nb, B0, B1, y + 1);  // A holds only z > y
-                    warp_chunks(a.nb, B0, B1, A0, A1, lane, search_x, chunk);
+                    warp_hits(a, B0, B1, x, A0, A1, lane, chunk);
                 } else {
-                    auto search_y = [&](int64_t lo, int64_t hi, int32_t v) { return row_lower_bound(a, y, lo, hi, v); };
-                    warp_chunks(a.nb, A0, A1, B0, B1, lane, search_y, chunk);
+                    warp_hits(a, A0, A1, y, B0, B1, lane, chunk);
                 }
                 if (owner && lane == 0) a.pe[i] = peacc;
             }
@@ -267,12 +228,11 @@ __global__ void __launch_bounds__(kHubBlock) k_rows_hub(RowsArgs a, const int32_
                     for (int64_t k0 = 0; k0 < L; k0 += 32) {
                         const double vn = k0 + 32 + lane < L ? rg[k0 + 32 + lane] : 0.0;  // next 32, ahead of the chain
                         const int c = L - k0 < 32 ? (int)(L - k0) : 32;
-                        double t[32];
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) t[j] = __shfl_sync(0xffffffffu, v, j);
-#pragma unroll
-                        for (int j = 0; j < 32; ++j)
-                            if (j < c) pvacc += t[j];
+                        for (int j = 0; j < 32; ++j) {
+                            const double t = __shfl_sync(0xffffffffu, v, j);
+                            if (j < c) pvacc += t;
+                        }
                         v = vn;
                     }
                 }
@@ -294,49 +254,120 @@ __global__ void k_hub_keys(const int32_t* __restrict__ deg, int64_t n, int hub, 
             keys[atomicAdd(nh, 1u)] = ((uint64_t)(0x7fffffff - deg[v]) << 32) | (uint64_t)v;
 }
 
-__global__ void k_hub_index_sizes(const int32_t* __restrict__ hubs, int64_t nh, const int32_t* __restrict__ deg,
-                                  int32_t* __restrict__ hub_pos, int64_t* __restrict__ cnt)
-{
-    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h <= nh; h += (int64_t)gridDim.x * blockDim.x) {
-        if (h == nh) {
-            cnt[h] = 0;
-            continue;
-        }
-        hub_pos[hubs[h]] = (int32_t)h;
-        cnt[h] = (deg[hubs[h]] + kIdxStride - 1) / kIdxStride;
-    }
-}
-
-// A warp per hub (dealt modulo the warp count): sample k of hub h is its row's entry kIdxStride*k.
-__global__ void k_hub_index_fill(const int32_t* __restrict__ hubs, int64_t nh, const int64_t* __restrict__ off,
-                                 const int32_t* __restrict__ nb, const int64_t* __restrict__ ioff,
-                                 int32_t* __restrict__ idx)
-{
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x / 32);
-    for (int64_t h = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; h < nh; h += nwarps) {
-        const int64_t x = hubs[h], base = off[x];
-        const int64_t cnt = ioff[h + 1] - ioff[h];
-        for (int64_t k = lane; k < cnt; k += 32) idx[ioff[h] + k] = nb[base + k * kIdxStride];
-    }
-}
-
 __global__ void k_hub_ids(const uint64_t* __restrict__ keys, int64_t nh, int32_t* __restrict__ ids)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nh; i += (int64_t)gridDim.x * blockDim.x)
         ids[i] = (int32_t)(keys[i] & 0xffffffffu);
 }
 
+// Row sets: the vertices of at least min_deg neighbours, numbered in id order
+// (flag + scan), each with a power-of-two table of >= 2 deg slots.
+__global__ void k_rs_flags(const int32_t* __restrict__ deg, int64_t n, int min_deg, int64_t* __restrict__ flag)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v <= n; v += (int64_t)gridDim.x * blockDim.x)
+        flag[v] = (v < n && deg[v] >= min_deg) ? 1 : 0;
+}
+
+__global__ void k_rs_sizes(const int32_t* __restrict__ deg, int64_t n, const int64_t* __restrict__ num,
+                           int32_t* __restrict__ tab, int32_t* __restrict__ owner, int32_t* __restrict__ tbits,
+                           int64_t* __restrict__ tsize)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        if (num[v + 1] == num[v]) {
+            tab[v] = -1;
+            continue;
+        }
+        const int32_t t = (int32_t)num[v];
+        int bits = 1;
+        while ((1ll << bits) < 2ll * deg[v]) ++bits;
+        tab[v] = t;
+        owner[t] = (int32_t)v;
+        tbits[t] = bits;
+        tsize[t] = 1ll << bits;
+    }
+}
+
+// A warp per table (dealt modulo the warp count) inserts its row; the table
+// is at least half empty, so every probe sequence meets an empty slot.
+__global__ void k_rs_insert(const int32_t* __restrict__ owner, int64_t nt, const int64_t* __restrict__ off,
+                            const int32_t* __restrict__ nb, const int64_t* __restrict__ toff,
+                            const int32_t* __restrict__ tbits, int32_t* __restrict__ slot)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x / 32);
+    for (int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; t < nt; t += nwarps) {
+        const int32_t v = owner[t];
+        const int bits = tbits[t];
+        const uint32_t mask = (1u << bits) - 1u;
+        int32_t* tb = slot + toff[t];
+        for (int64_t p = off[v] + lane; p < off[v + 1]; p += 32) {
+            const int32_t z = nb[p];
+            uint32_t h = rs_hash(z, bits);
+            while (atomicCAS(&tb[h], -1, z) != -1) h = (h + 1u) & mask;
+        }
+    }
+}
+
 }  // namespace
+
+// Hash sets of every row of at least min_deg entries, in scratch (live until
+// sc is released); *out stays empty when no row qualifies.
+int build_row_sets(rtr_graph* g, Scratch& sc, int min_deg, RowSets* out)
+{
+    *out = RowSets{nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t s = g->stream;
+    const int64_t n = g->n;
+    int64_t* flag = (int64_t*)sc.get(sizeof(int64_t) * (n + 1));
+    int64_t* num = (int64_t*)sc.get(sizeof(int64_t) * (n + 1));
+    int64_t* tmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(n + 1));
+    int32_t* tab = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
+    if (!flag || !num || !tmp || !tab) {
+        set_error("device allocation failed (row sets)");
+        return RTR_ERR_CUDA;
+    }
+    k_rs_flags<<<grid_for(n + 1, 256), 256, 0, s>>>(g->deg, n, min_deg, flag);
+    exclusive_scan_i64(flag, num, n + 1, nullptr, tmp, s);
+    int64_t nt = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&nt, num + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    g->launches += 2;
+    if (nt == 0) return RTR_OK;
+    int32_t* owner = (int32_t*)sc.get(sizeof(int32_t) * (nt + 1));
+    int32_t* tbits = (int32_t*)sc.get(sizeof(int32_t) * (nt + 1));
+    int64_t* tsize = (int64_t*)sc.get(sizeof(int64_t) * (nt + 1));
+    int64_t* toff = (int64_t*)sc.get(sizeof(int64_t) * (nt + 1));
+    int64_t* ltmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(nt + 1));
+    if (!owner || !tbits || !tsize || !toff || !ltmp) {
+        set_error("device allocation failed (row sets)");
+        return RTR_ERR_CUDA;
+    }
+    RTR_CUDA_TRY(cudaMemsetAsync(tsize + nt, 0, sizeof(int64_t), s));
+    k_rs_sizes<<<grid_for(n, 256), 256, 0, s>>>(g->deg, n, num, tab, owner, tbits, tsize);
+    exclusive_scan_i64(tsize, toff, nt + 1, nullptr, ltmp, s);
+    int64_t total = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&total, toff + nt, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaStreamSynchronize(s));
+    int32_t* slot = (int32_t*)sc.get(sizeof(int32_t) * (total + 1));
+    if (!slot) {
+        set_error("device allocation failed (row sets: %lld slots)", (long long)total);
+        return RTR_ERR_CUDA;
+    }
+    RTR_CUDA_TRY(cudaMemsetAsync(slot, 0xff, sizeof(int32_t) * (total + 1), s));
+    k_rs_insert<<<grid_for(1ll << 40, 256, 8), 256, 0, s>>>(owner, nt, g->offsets, g->nbors, toff, tbits, slot);
+    g->launches += 3;
+    RTR_CUDA_TRY(cudaGetLastError());
+    *out = RowSets{tab, toff, tbits, slot};
+    return RTR_OK;
+}
 
 // perVertex (all vertices) and heavy-edge perEdge from the rows; the caller has
 // run the edge fold and heavy-edge count.  Synchronises the graph's stream.
-int count_rows(rtr_graph* g, Scratch& sc)
+int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs)
 {
     cudaStream_t s = g->stream;
     const int64_t n = g->n;
     RowsArgs a{g->offsets, g->nbors, g->deg, n, g->pe, g->pv, g->tune_gallop, g->tune_edge, g->tune_heavy,
-               g->count_hub, nullptr, nullptr, nullptr};
+               g->count_hub, rs};
     if (a.hub < a.light) a.hub = a.light;
     uint64_t* keys = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
     uint64_t* alt = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
@@ -371,7 +402,8 @@ int count_rows(rtr_graph* g, Scratch& sc)
         cap = (int64_t)(0x7fffffff - (int64_t)(first >> 32));  // the largest hub degree
         int dev_sms = 148;
         cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device);
-        hub_grid = (int)((int64_t)nh < dev_sms ? (int64_t)nh : dev_sms);
+        const int64_t want = 2ll * dev_sms;  // two hub blocks per SM
+        hub_grid = (int)((int64_t)nh < want ? (int64_t)nh : want);
         hbuf = (double*)sc.get(sizeof(double) * (size_t)hub_grid * 2 * (kHubWarps - 1) * (size_t)(cap + 32));
         if (!hbuf) {
             set_error("device allocation failed (hub fold buffers, %lld hubs of degree up to %lld)", (long long)nh,
@@ -379,32 +411,6 @@ int count_rows(rtr_graph* g, Scratch& sc)
             return RTR_ERR_CUDA;
         }
         cap += 32;
-        // the hubs' sample index
-        int32_t* hub_pos = (int32_t*)sc.get(sizeof(int32_t) * (n + 1));
-        int64_t* icnt = (int64_t*)sc.get(sizeof(int64_t) * (nh + 1));
-        int64_t* ioff = (int64_t*)sc.get(sizeof(int64_t) * (nh + 1));
-        int64_t* itmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(nh + 1));
-        int64_t* itot = (int64_t*)sc.get(sizeof(int64_t) * 2);
-        if (!hub_pos || !icnt || !ioff || !itmp || !itot) {
-            set_error("device allocation failed (hub index)");
-            return RTR_ERR_CUDA;
-        }
-        RTR_CUDA_TRY(cudaMemsetAsync(hub_pos, 0xff, sizeof(int32_t) * (n + 1), s));
-        k_hub_index_sizes<<<grid_for(nh, 256), 256, 0, s>>>(hubs, nh, g->deg, hub_pos, icnt);
-        exclusive_scan_i64(icnt, ioff, nh + 1, itot, itmp, s);
-        int64_t ntot = 0;
-        RTR_CUDA_TRY(cudaMemcpyAsync(&ntot, itot, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        RTR_CUDA_TRY(cudaStreamSynchronize(s));
-        int32_t* idx = (int32_t*)sc.get(sizeof(int32_t) * (ntot + 1));
-        if (!idx) {
-            set_error("device allocation failed (hub index)");
-            return RTR_ERR_CUDA;
-        }
-        k_hub_index_fill<<<grid_for(1ll << 40, 256, 8), 256, 0, s>>>(hubs, nh, g->offsets, g->nbors, ioff, idx);
-        g->launches += 5;
-        a.hub_pos = hub_pos;
-        a.idx_off = ioff;
-        a.idx = idx;
     }
     cudaEvent_t ready = nullptr, joined = nullptr;
     if (hub_grid > 0) {

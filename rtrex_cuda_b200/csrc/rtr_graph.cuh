@@ -151,7 +151,11 @@ struct Scratch {
 int build_csr(rtr_graph* g, const int64_t* d_u, const int64_t* d_v, int64_t m, bool simplify);
 int build_csr_from_host_csr(rtr_graph* g, const int64_t* h_offsets, const int64_t* h_nbors);
 int count_triangles(rtr_graph* g);
-int count_rows(rtr_graph* g, Scratch& sc);  // list-free perVertex / heavy perEdge (count_rows.cu)
+struct RowSets;
+// hash sets of the rows of at least min_deg entries, in sc (count_rows.cu)
+int build_row_sets(rtr_graph* g, Scratch& sc, int min_deg, RowSets* out);
+// list-free perVertex / heavy perEdge (count_rows.cu)
+int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs);
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 int initial_clean(rtr_graph* g, double eps);
 int extract_clusters(rtr_graph* g);
