@@ -330,12 +330,13 @@ class Graph:
         return {"ms_build": ms[0], "ms_count": ms[1], "ms_clean": ms[2], "ms_extract": ms[3],
                 "launches": int(launches.value), "residual_warnings": int(resid.value)}
 
-    KERNELS = ("k_edge_fold", "k_tri_fill", "k_vertex_fold", "k_clean_units", "k_extract_components", "decompose")
+    KERNELS = ("k_edge_fold", "k_tri_fill", "k_vertex_fold", "k_clean_units", "k_extract_components", "decompose",
+               "k_rows_light", "k_rows_medium", "k_rows_hub")
 
     def kernel_ms(self) -> dict:
         """Device times (ms) of the last run's main kernels and of the whole decompose."""
-        ms = np.zeros(8, np.float64)
-        _check(lib().rtr_get_kernel_ms(self._h, _ptr(ms), 8))
+        ms = np.zeros(len(self.KERNELS), np.float64)
+        _check(lib().rtr_get_kernel_ms(self._h, _ptr(ms), len(self.KERNELS)))
         return {k: float(ms[i]) for i, k in enumerate(self.KERNELS)}
 
     def write_decomposition(self, name: str):

@@ -419,12 +419,18 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs)
         RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
         RTR_CUDA_TRY(cudaEventRecord(ready, s));
         RTR_CUDA_TRY(cudaStreamWaitEvent(g->side, ready, 0));
+        ktime_begin(g, KT_ROWS_HUB, g->side);
         k_rows_hub<<<hub_grid, kHubBlock, 0, g->side>>>(a, hubs, nh, hbuf, cap);
+        ktime_end(g, KT_ROWS_HUB, g->side);
         RTR_CUDA_TRY(cudaEventRecord(joined, g->side));
         g->launches += 1;
     }
+    ktime_begin(g, KT_ROWS_LIGHT);
     k_rows_light<<<grid_for(n, kLightBlock), kLightBlock, 0, s>>>(a);
+    ktime_end(g, KT_ROWS_LIGHT);
+    ktime_begin(g, KT_ROWS_MEDIUM);
     k_rows_medium<<<grid_for(1ll << 40, kMediumBlock, 16), kMediumBlock, 0, s>>>(a);
+    ktime_end(g, KT_ROWS_MEDIUM);
     g->launches += 2;
     cudaError_t e = cudaGetLastError();
     if (joined) {
@@ -432,7 +438,13 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs)
         cudaStreamSynchronize(s);  // scratch (hub list, buffers) is freed on return
         cudaEventDestroy(ready);
         cudaEventDestroy(joined);
+        ktime_read(g, KT_ROWS_HUB);
+    } else {
+        g->kms[KT_ROWS_HUB] = 0;
     }
+    cudaStreamSynchronize(s);
+    ktime_read(g, KT_ROWS_LIGHT);
+    ktime_read(g, KT_ROWS_MEDIUM);
     if (e != cudaSuccess) return cuda_fail(e, "rows-layout counting launch", __FILE__, __LINE__);
     return RTR_OK;
 }

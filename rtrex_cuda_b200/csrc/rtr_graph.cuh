@@ -106,7 +106,9 @@ struct rtr_graph {
     float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0, ms_decompose = 0, ms_expand = 0;
     // per-kernel device times of the last run (ms), CUDA events on the graph's stream:
     // [0] k_edge_fold [1] k_tri_fill [2] k_vertex_fold [3] k_clean_units [4] k_extract_components
-    static constexpr int kTimers = 8;
+    // [5] decompose [6] k_rows_light [7] k_rows_medium [8] k_rows_hub (rows layout; the hub
+    // kernel on the second stream, concurrent with the other two)
+    static constexpr int kTimers = 10;
     cudaEvent_t kev[2 * kTimers] = {};
     float kms[kTimers] = {};
     // launch accounting for this graph (kernels issued by the library)
@@ -128,9 +130,25 @@ namespace rtr {
 void* dev_alloc(rtr_graph* g, size_t bytes);  // stream-ordered, owned by g
 
 // Kernel timers: record around a launch on the graph's stream, read after a sync.
-enum KernelTimer { KT_EDGE_FOLD = 0, KT_TRI_FILL, KT_VERTEX_FOLD, KT_CLEAN_UNITS, KT_EXTRACT, KT_DECOMPOSE };
-inline void ktime_begin(rtr_graph* g, int k) { cudaEventRecord(g->kev[2 * k], g->stream); }
-inline void ktime_end(rtr_graph* g, int k) { cudaEventRecord(g->kev[2 * k + 1], g->stream); }
+enum KernelTimer {
+    KT_EDGE_FOLD = 0,
+    KT_TRI_FILL,
+    KT_VERTEX_FOLD,
+    KT_CLEAN_UNITS,
+    KT_EXTRACT,
+    KT_DECOMPOSE,
+    KT_ROWS_LIGHT,
+    KT_ROWS_MEDIUM,
+    KT_ROWS_HUB
+};
+inline void ktime_begin(rtr_graph* g, int k, cudaStream_t s = nullptr)
+{
+    cudaEventRecord(g->kev[2 * k], s ? s : g->stream);
+}
+inline void ktime_end(rtr_graph* g, int k, cudaStream_t s = nullptr)
+{
+    cudaEventRecord(g->kev[2 * k + 1], s ? s : g->stream);
+}
 inline void ktime_read(rtr_graph* g, int k)
 {
     float ms = 0;
