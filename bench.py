@@ -349,9 +349,10 @@ def rmat24_leg(args, dev, flush_l2, peak, peak_kind, scale=24, steps=None, mode=
            "n": n, "m": m, "triangles": total, "layout": layout, "steps": steps,
            "ms_per_count": t * 1e3, "edges_per_s": m / t, "triangles_per_s": total / t,
            "generation_and_csr_build_ms": gen_ms,
-           "kernel_ms": {"edge_fold_and_heavy_count": kms["k_edge_fold"], "rows_folds": kms["k_vertex_fold"],
-                         "rows_light": kms["k_rows_light"], "rows_medium": kms["k_rows_medium"],
-                         "rows_hub": kms["k_rows_hub"]},
+           "kernel_ms": {"edge_fold_and_heavy_count": kms["k_edge_fold"],
+                         "edge_fold_light_edges": kms["k_edge_fold_light"],
+                         "edge_count_heavy_edges": kms["k_edge_count_heavy"], "list_fill": kms["k_tri_fill"],
+                         "vertex_fold": kms["k_vertex_fold"], "vertex_fold_warps": kms["k_vfold_warp"]},
            "gpu_launches_per_count": launches,
            "roofline_count": {"bound": "hbm", "algorithmic_bytes": b_count, "oriented_sum": osum,
                               "achieved": b_count / t / 1e9, "peak": peak, "unit": "GB/s",

@@ -122,10 +122,12 @@ int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int
  * (32 B per triangle and edge) when they fit in the device memory that is free
  * beside what the clean needs, and otherwise counts without them; mode 1 always
  * keeps them (RTR_ERR_CUDA when they do not fit); mode 2 never does.  Without
- * lists ("rows layout") perVertex and the perEdge of heavy edges are folded
- * straight from the CSR rows -- the same bits -- and vertices of at least
- * hub_degree neighbours (default 4096) are folded by a whole thread block; the
- * clean and the extraction need the lists, so rtr_clean then returns
+ * them ("rows layout") the count keeps 4-byte per-slot lists of the z > y terms
+ * of perVertex instead (taken in windows of whole rows when even those do not
+ * fit) and folds perVertex from them -- the same bits; a vertex of at least
+ * hub_degree perVertex terms (default 1024) is folded by a warp, the others by
+ * a thread.  The clean and the extraction need the triangle lists, so
+ * rtr_clean then returns
  * RTR_ERR_LIMIT.  *lists_kept tells whether the last rtr_count kept them.  No
  * counterpart in the reference, whose commonNbr keeps no lists
  * (RTRex_Sequential/Escape/Decomposition.h:42-117). */

@@ -331,7 +331,7 @@ class Graph:
                 "launches": int(launches.value), "residual_warnings": int(resid.value)}
 
     KERNELS = ("k_edge_fold", "k_tri_fill", "k_vertex_fold", "k_clean_units", "k_extract_components", "decompose",
-               "k_rows_light", "k_rows_medium", "k_rows_hub")
+               "k_edge_fold_light", "k_edge_count_heavy", "k_vfold_warp")
 
     def kernel_ms(self) -> dict:
         """Device times (ms) of the last run's main kernels and of the whole decompose."""
@@ -346,11 +346,12 @@ class Graph:
         """Counting work split (results are identical for every setting)."""
         _check(lib().rtr_set_tuning(self._h, int(gallop_ratio), int(heavy_degree), int(heavy_edge)))
 
-    def set_count_mode(self, mode: int, hub_degree: int = 4096):
+    def set_count_mode(self, mode: int, hub_degree: int = 1024):
         """Counting layout: 0 keep triangle lists when they fit (default), 1 always,
-        2 never (rows layout: folds straight from the CSR rows; same bits, but the
-        clean needs the lists).  Vertices of at least hub_degree neighbours are
-        folded by a thread block in the rows layout."""
+        2 never (rows layout: 4-byte per-slot lists of z instead of the 32-byte
+        triangle entries; same bits, but the clean needs the lists).  In the rows
+        layout a vertex of at least hub_degree perVertex terms is folded by a warp,
+        the others by a thread."""
         _check(lib().rtr_set_count_mode(self._h, int(mode), int(hub_degree)))
 
     def count_mode(self):

@@ -51,11 +51,16 @@ __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned lon
     }
 }
 
+// cgt (may be null): for each directed slot (x,y), the number of common
+// neighbours z > y -- the terms slot (x,y) adds to perVertex[x] -- written for
+// both slots of every edge (the rows layout's list offsets).
 __global__ void __launch_bounds__(kBlock)
     k_edge_fold(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
-                const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd, int64_t m, double* __restrict__ pe,
-                uint32_t* __restrict__ sup, int64_t* __restrict__ cnt, unsigned long long* __restrict__ total,
-                int gallop, int heavy_edge, int32_t* __restrict__ heavy_list, unsigned* __restrict__ nheavy)
+                const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd,
+                const int32_t* __restrict__ partner, int64_t m, RowSets rs, double* __restrict__ pe,
+                uint32_t* __restrict__ sup, int64_t* __restrict__ cnt, int64_t* __restrict__ cgt,
+                unsigned long long* __restrict__ total, int gallop, int heavy_edge, int32_t* __restrict__ heavy_list,
+                unsigned* __restrict__ nheavy)
 {
     unsigned long long tri = 0;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
@@ -67,15 +72,20 @@ __global__ void __launch_bounds__(kBlock)
         }
         const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
         double acc = 0.0;
-        uint32_t c = 0, above = 0;
-        intersect_rows(nb, off[u], off[u + 1], off[v], off[v + 1], gallop, [&](int32_t z, int64_t, int64_t) {
+        uint32_t c = 0, above = 0, above_u = 0;
+        thread_common(rs, off, nb, u, v, INT32_MIN, gallop, [&](int32_t z) {
             acc += 1.0 / (double)(duv * (int64_t)deg[z]);
             ++c;
             above += (z > v) ? 1u : 0u;
+            above_u += (z > u) ? 1u : 0u;
         });
         pe[i] = acc;
         sup[i] = c;
         cnt[i] = c;
+        if (cgt) {
+            cgt[i] = above;
+            cgt[partner[i]] = above_u;
+        }
         tri += above;
     }
     block_add_u64(tri, total);
@@ -115,42 +125,61 @@ __global__ void __launch_bounds__(kBlock)
 // (the same left fold over z ascending as the thread path).
 constexpr int kHeavyEdgeBlock = 128;
 
+// pe (may be null): also fold perEdge of the heavy edges, in ascending z, from
+// an ordered walk of the shorter row (the lists layout folds them from the
+// lists instead, k_pe_fold_heavy).  cgt as in k_edge_fold.
 __global__ void __launch_bounds__(kHeavyEdgeBlock)
     k_edge_count_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
-                       const int32_t* __restrict__ fwd, const int32_t* __restrict__ heavy_list,
+                       const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd,
+                       const int32_t* __restrict__ partner, const int32_t* __restrict__ heavy_list,
                        const unsigned* __restrict__ nheavy, int gallop, RowSets rs, uint32_t* __restrict__ sup,
-                       int64_t* __restrict__ cnt, unsigned long long* __restrict__ total)
+                       int64_t* __restrict__ cnt, int64_t* __restrict__ cgt, double* __restrict__ pe,
+                       unsigned long long* __restrict__ total)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ double s_w[kHeavyEdgeBlock / 32][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t nh = *nheavy;
     const int64_t nwarps = (int64_t)gridDim.x * (kHeavyEdgeBlock / 32);
     unsigned long long tri = 0;
-    for (int64_t h = (int64_t)blockIdx.x * (kHeavyEdgeBlock / 32) + (threadIdx.x >> 5); h < nh; h += nwarps) {
+    for (int64_t h = (int64_t)blockIdx.x * (kHeavyEdgeBlock / 32) + wib; h < nh; h += nwarps) {
         const int64_t i = fwd[heavy_list[h]];
         const int32_t u = esrc[i], v = nb[i];
         const int64_t u0 = off[u], u1 = off[u + 1], v0 = off[v], v1 = off[v + 1];
-        unsigned c = 0, above = 0;
-        // the shorter row walked against the longer one's hash set, when it has one
+        unsigned c = 0, above = 0, above_u = 0;
+        // the shorter row walked against the longer one
         const bool u_short = u1 - u0 <= v1 - v0;
         const int32_t t = rs_table(rs, u_short ? v : u);
-        if (t >= 0) {
-            const int32_t zmax = u_short ? nb[v1 - 1] : nb[u1 - 1];
-            warp_scan(nb, u_short ? u0 : v0, u_short ? u1 : v1, zmax, lane,
-                      [&](int32_t z) { return rs_member(rs, t, z); }, [&](bool hit, int32_t z) {
+        if (pe || t >= 0) {
+            const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
+            double acc = 0.0;
+            warp_walk(rs, off, nb, u_short ? u0 : v0, u_short ? u1 : v1, u_short ? v : u, u_short ? v0 : u0,
+                      u_short ? v1 : u1, lane, [&](bool hit, int32_t z) {
                           c += hit ? 1u : 0u;
                           above += (hit && z > v) ? 1u : 0u;
+                          above_u += (hit && z > u) ? 1u : 0u;
+                          if (pe) {
+                              const double w = hit ? 1.0 / (double)(duv * (int64_t)deg[z]) : 0.0;
+                              fold_hits(hit, w, s_w[wib], lane, &acc, nullptr, 0);
+                          }
                       });
+            if (pe && lane == 0) pe[i] = acc;
         } else {
             warp_intersect_part(nb, u0, u1, v0, v1, gallop, lane, [&](int32_t z, int64_t, int64_t) {
                 ++c;
                 above += (z > v) ? 1u : 0u;
+                above_u += (z > u) ? 1u : 0u;
             });
         }
         c = __reduce_add_sync(0xffffffffu, c);
         above = __reduce_add_sync(0xffffffffu, above);
+        above_u = __reduce_add_sync(0xffffffffu, above_u);
         if (lane == 0) {
             sup[i] = c;
             cnt[i] = c;
+            if (cgt) {
+                cgt[i] = above;
+                cgt[partner[i]] = above_u;
+            }
             tri += above;
         }
     }
@@ -366,10 +395,27 @@ int count_triangles(rtr_graph* g)
         const int rc = build_row_sets(g, sc, kSetDegree, &rs);
         if (rc) return rc;
     }
-    k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, m, g->pe, g->sup, cnt, g->ctr,
-                                      g->tune_gallop, g->tune_edge, heavy_list, nheavy);
-    k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->fwd, heavy_list, nheavy,
-                                                      g->tune_gallop, rs, g->sup, cnt, g->ctr);
+    // per-slot counts of perVertex terms, for the rows layout's lists
+    int64_t* cgt = nullptr;
+    if (g->count_mode != 1) {
+        cgt = (int64_t*)sc.get(sizeof(int64_t) * (m2 + 1));
+        if (!cgt) {
+            set_error("device allocation failed (count scratch)");
+            return RTR_ERR_CUDA;
+        }
+        RTR_CUDA_TRY(cudaMemsetAsync(cgt, 0, sizeof(int64_t) * (m2 + 1), s));
+    }
+    // heavy-edge perEdge folded by the count when the rows layout is likely
+    const bool heavy_pe = g->count_mode == 2 || rs.tab != nullptr;
+    ktime_begin(g, KT_EDGE_LIGHT);
+    k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, g->partner, m, rs, g->pe,
+                                      g->sup, cnt, cgt, g->ctr, g->tune_gallop, g->tune_edge, heavy_list, nheavy);
+    ktime_end(g, KT_EDGE_LIGHT);
+    ktime_begin(g, KT_EDGE_HEAVY);
+    k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, g->partner,
+                                                      heavy_list, nheavy, g->tune_gallop, rs, g->sup, cnt, cgt,
+                                                      heavy_pe ? g->pe : nullptr, g->ctr);
+    ktime_end(g, KT_EDGE_HEAVY);
     ktime_end(g, KT_EDGE_FOLD);
     exclusive_scan_i64(cnt, g->tl_off, m2 + 1, nullptr, tmp, s);
     g->launches += 6;
@@ -390,19 +436,27 @@ int count_triangles(rtr_graph* g)
         // rows layout: perVertex and heavy-edge perEdge straight from the CSR rows
         g->lists = false;
         g->tl_len = 0;
-        ktime_begin(g, KT_TRI_FILL);
-        ktime_end(g, KT_TRI_FILL);
-        ktime_begin(g, KT_VERTEX_FOLD);
-        const int rc = count_rows(g, sc, rs);
-        ktime_end(g, KT_VERTEX_FOLD);
+        if (!heavy_pe) {  // fold the heavy edges' perEdge now (the counts are recomputed, unchanged)
+            unsigned long long* junk = (unsigned long long*)sc.get(sizeof(unsigned long long) * 2);
+            if (!junk) {
+                set_error("device allocation failed (count scratch)");
+                return RTR_ERR_CUDA;
+            }
+            k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd,
+                                                              g->partner, heavy_list, nheavy, g->tune_gallop, rs,
+                                                              g->sup, cnt, nullptr, g->pe, junk);
+            g->launches += 1;
+        }
+        // cnt (scanned into tl_off above) is free: it takes the lists' offsets
+        const int rc = count_rows(g, sc, rs, cgt, cnt, heavy_list, nheavy);
         if (rc) return rc;
         RTR_CUDA_TRY(cudaGetLastError());
         cudaEventRecord(e1, s);
         RTR_CUDA_TRY(cudaEventSynchronize(e1));
         cudaEventElapsedTime(&g->ms_count, e0, e1);
         ktime_read(g, KT_EDGE_FOLD);
-        ktime_read(g, KT_TRI_FILL);
-        ktime_read(g, KT_VERTEX_FOLD);
+        ktime_read(g, KT_EDGE_LIGHT);
+        ktime_read(g, KT_EDGE_HEAVY);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         g->stage = 2;
@@ -437,6 +491,8 @@ int count_triangles(rtr_graph* g)
     RTR_CUDA_TRY(cudaEventSynchronize(e1));
     cudaEventElapsedTime(&g->ms_count, e0, e1);
     ktime_read(g, KT_EDGE_FOLD);
+    ktime_read(g, KT_EDGE_LIGHT);
+    ktime_read(g, KT_EDGE_HEAVY);
     ktime_read(g, KT_TRI_FILL);
     ktime_read(g, KT_VERTEX_FOLD);
     cudaEventDestroy(e0);

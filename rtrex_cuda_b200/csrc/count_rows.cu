@@ -1,39 +1,36 @@
-// List-free weighted triangle counting ("rows" layout): perVertex and the
-// perEdge of heavy edges folded straight from the CSR rows, with no
-// per-triangle storage, for graphs whose triangle lists do not fit in HBM
-// (R-MAT scale 22 already has 2.1 G triangles, i.e. ~200 GB of lists; scale 24
-// 10.3 G).  commonNbr itself keeps no lists either
-// (RTRex_Sequential/Escape/Decomposition.h:70-115): it re-intersects rows.
+// Weighted triangle counting without TriEntry lists ("rows" layout), for
+// graphs whose 32-byte-per-entry triangle lists do not fit in HBM (R-MAT
+// scale 22 has 2.1 G triangles, ~200 GB of lists; scale 24 10.3 G).
+// commonNbr itself keeps no lists (RTRex_Sequential/Escape/Decomposition.h:
+// 70-115); its two ordered folds are
+//   perEdge[(x,y)] = left fold over z in N(x) & N(y) ascending of w(x,y,z)
+//   perVertex[x]   = left fold over y in N(x) ascending, then over
+//                    z in N(x) & N(y), z > y ascending, of w(x,y,z)
+// with w(x,y,z) = 1/double(dx*dy*dz).
 //
-// What runs before this (count.cu): k_edge_fold folds perEdge for every light
-// edge (deg u + deg v below the heavy-edge threshold) and k_edge_count_heavy
-// counts the heavy ones, so support, the triangle total and light perEdge are
-// known.  This file adds, bit-exact to commonNbr's discovery order:
-//   perVertex[x] = left fold over y in N(x) ascending, then over
-//                  z in N(x) & N(y), z > y ascending, of 1/double(dx*dy*dz)
-//   perEdge[(x,y)] for heavy edges, x < y = left fold over z in N(x) & N(y)
-//                  ascending, computed by x's pass from the same intersection.
-// For y > x owning a heavy edge the pass intersects the full rows (perEdge
-// needs every z; the z > y suffix continues perVertex[x]); otherwise it
-// intersects N(x) beyond y with N(y).  Every intersection walks the shorter
-// range in ascending order and looks its elements up in the longer row: in that
-// row's hash set when it has one (rowsets.cuh; build_row_sets below makes one
-// for every row of at least kSetDegree entries), else by binary search.
-//
-// Three kernels by the degree of x:
-//   k_rows_light   a thread per vertex of degree < light
-//   k_rows_medium  a warp per vertex of degree in [light, hub): for each y in
-//                  turn the warp walks the shorter range 32 elements at a time
-//                  and folds the hits in lane order (ascending z)
-//   k_rows_hub     a thread block per vertex of degree >= hub, hubs in
-//                  descending degree, two blocks per SM: 7 producer warps take
-//                  7 consecutive y at once, each writing its y's z > y weights,
-//                  in order, to its own buffer, which warp 0 folds in y order
-//                  while the producers work on the next 7 (double-buffered) --
-//                  only the perVertex chain itself is sequential.
-// The hub kernel runs on the graph's second stream, concurrently with the
-// other two (it holds the longest dependent chain: ~10^8 adds for the largest
-// R-MAT scale-24 hub).
+// What runs before this (count.cu): one intersection per undirected edge
+// gives support, the triangle total, perEdge (light edges by a thread, heavy
+// ones by a warp walking the shorter row in order) and, for every directed
+// slot (x,y), cgt = #{z in N(x) & N(y) : z > y} -- the number of terms slot
+// (x,y) adds to perVertex[x].  This file makes perVertex from that:
+//   lists     the exclusive scan of cgt gives every slot a list of its z > y,
+//             4 bytes each (3 per triangle: ~124 GB at R-MAT scale 24).
+//             Slots are taken in windows of whole rows that fit in the free
+//             HBM (one window when everything fits).
+//   fill      one more intersection per edge (u < v) restricted to z > u
+//             writes both slots' lists in ascending z: z > u to slot (v,u),
+//             z > v to slot (u,v).  k_fill_light: a thread per light edge;
+//             k_fill_heavy: a warp per heavy edge, hits ranked by ballot.
+//   fold      perVertex[x] = the left fold of x's slots' lists in slot order
+//             (y ascending), each in z order -- exactly commonNbr's order.
+//             k_vfold_thread: a thread per vertex of few terms;
+//             k_vfold_warp: a warp per vertex of at least `warp_min` terms,
+//             vertices dealt from a queue in descending term count, the
+//             weights of 32 terms computed by the lanes and added in lane
+//             order (the one sequential part: ~10^8 adds for the largest
+//             R-MAT scale-24 hub).
+// Membership lookups use the hash sets of the long rows (rowsets.cuh,
+// build_row_sets below).
 #include "intersect.cuh"
 #include "primitives.cuh"
 #include "rowsets.cuh"
@@ -43,221 +40,208 @@ namespace rtr {
 
 namespace {
 
-constexpr int kLightBlock = 256;
-constexpr int kMediumBlock = 128;
-constexpr int kHubWarps = 8;
-constexpr int kHubBlock = 32 * kHubWarps;
+constexpr int kFillBlock = 256;
+constexpr int kHeavyBlock = 128;
+constexpr int kFoldBlock = 256;
 
-struct RowsArgs {
+struct FillArgs {
+    const int64_t* off;
+    const int32_t* nb;
+    const int32_t* esrc;
+    const int32_t* partner;
+    const int32_t* deg;
+    const int32_t* fwd;
+    int64_t m;
+    int heavy_edge;
+    int gallop;
+    RowSets rs;
+    const int64_t* lpos;  // [m2+1] first list entry of every slot (all windows numbered together)
+    int64_t p0, p1;       // the window's slots
+    int64_t e0;           // lpos[p0]: entry e of the window lives at lists[e - e0]
+    int32_t* lists;
+};
+
+__device__ __forceinline__ bool in_window(const FillArgs& a, int64_t p) { return p >= a.p0 && p < a.p1; }
+
+// Light edges (deg u + deg v below heavy_edge), a thread each.
+__global__ void __launch_bounds__(kFillBlock) k_fill_light(FillArgs a)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < a.m; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = a.fwd[k];
+        const int32_t u = a.esrc[i], v = a.nb[i];
+        if (a.deg[u] + a.deg[v] >= a.heavy_edge) continue;
+        const int64_t r = a.partner[i];
+        const bool wi = in_window(a, i), wr = in_window(a, r);
+        if (!wi && !wr) continue;
+        // each slot's list ends where the next begins: the writes stay inside it
+        int64_t qi = a.lpos[i] - a.e0, qr = a.lpos[r] - a.e0;
+        const int64_t qi1 = a.lpos[i + 1] - a.e0, qr1 = a.lpos[r + 1] - a.e0;
+        thread_common(a.rs, a.off, a.nb, u, v, wr ? u + 1 : v + 1, a.gallop, [&](int32_t z) {
+            if (wr && qr < qr1) a.lists[qr++] = z;
+            if (wi && z > v && qi < qi1) a.lists[qi++] = z;
+        });
+    }
+}
+
+// Heavy edges, a warp each, from the count's heavy-edge list.
+__global__ void __launch_bounds__(kHeavyBlock) k_fill_heavy(FillArgs a, const int32_t* __restrict__ heavy_list,
+                                                             const unsigned* __restrict__ nheavy)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t nh = *nheavy;
+    const int64_t nwarps = (int64_t)gridDim.x * (kHeavyBlock / 32);
+    for (int64_t h = (int64_t)blockIdx.x * (kHeavyBlock / 32) + (threadIdx.x >> 5); h < nh; h += nwarps) {
+        const int64_t i = a.fwd[heavy_list[h]];
+        const int32_t u = a.esrc[i], v = a.nb[i];
+        const int64_t r = a.partner[i];
+        const bool wi = in_window(a, i), wr = in_window(a, r);
+        if (!wi && !wr) continue;  // uniform across the warp
+        int64_t qi = a.lpos[i] - a.e0, qr = a.lpos[r] - a.e0;
+        const int64_t qi1 = a.lpos[i + 1] - a.e0, qr1 = a.lpos[r + 1] - a.e0;  // the writes stay inside each list
+        const int32_t from = wr ? u + 1 : v + 1;
+        const int64_t u0 = a.off[u], u1 = a.off[u + 1], v0 = a.off[v], v1 = a.off[v + 1];
+        const bool u_short = u1 - u0 <= v1 - v0;
+        const int64_t s1 = u_short ? u1 : v1;
+        const int64_t s0 = lower_bound_row(a.nb, u_short ? u0 : v0, s1, from);
+        warp_walk(a.rs, a.off, a.nb, s0, s1, u_short ? v : u, u_short ? v0 : u0, u_short ? v1 : u1, lane,
+                  [&](bool hit, int32_t z) {
+                      const bool to_r = hit && wr, to_i = hit && wi && z > v;
+                      const unsigned mr = __ballot_sync(0xffffffffu, to_r);
+                      const unsigned mi = __ballot_sync(0xffffffffu, to_i);
+                      const int64_t wr_at = qr + __popc(mr & lt), wi_at = qi + __popc(mi & lt);
+                      if (to_r && wr_at < qr1) a.lists[wr_at] = z;
+                      if (to_i && wi_at < qi1) a.lists[wi_at] = z;
+                      qr += __popc(mr);
+                      qi += __popc(mi);
+                  });
+    }
+}
+
+struct FoldArgs {
     const int64_t* off;
     const int32_t* nb;
     const int32_t* deg;
-    int64_t n;
-    double* pe;
+    const int64_t* lpos;
+    int64_t e0;
+    const int32_t* lists;
     double* pv;
-    int gallop;
-    int heavy_edge;  // deg x + deg y from which perEdge is folded here (k_edge_fold left it)
-    int light;       // vertices below this degree: a thread
-    int hub;         // vertices from this degree: a thread block
-    RowSets rs;
+    int64_t x0, x1;  // the window's vertices
+    int64_t warp_min;
 };
 
-__device__ __forceinline__ bool owns_heavy(const RowsArgs& a, int32_t x, int32_t y, int dx, int dy)
+__device__ __forceinline__ int64_t terms_of(const FoldArgs& a, int64_t x)
 {
-    return x < y && dx + dy >= a.heavy_edge;
+    return a.lpos[a.off[x + 1]] - a.lpos[a.off[x]];
 }
 
-// The warp's hits of the ascending range S = [s0, s1) in the range [l0, l1) of
-// row w: chunk(hit, z) per 32 elements of S, hits ascending.  Through w's hash
-// set when it has one -- exact because every caller passes either w's whole
-// row, or x's row cut just after y together with an S whose elements all
-// exceed y -- else by binary search.
-template <typename F>
-__device__ __forceinline__ void warp_hits(const RowsArgs& a, int64_t s0, int64_t s1, int32_t w, int64_t l0,
-                                          int64_t l1, int lane, F&& chunk)
+__global__ void __launch_bounds__(kFoldBlock) k_vfold_thread(FoldArgs a)
 {
-    const int32_t t = rs_table(a.rs, w);
-    if (t >= 0) {
-        const int32_t zmax = a.nb[a.off[w + 1] - 1];
-        warp_scan(a.nb, s0, s1, zmax, lane, [&](int32_t z) { return rs_member(a.rs, t, z); }, chunk);
-    } else {
-        warp_chunks(a.nb, s0, s1, l0, l1, lane,
-                    [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(a.nb, lo, hi, v); }, chunk);
-    }
-}
-
-__global__ void __launch_bounds__(kLightBlock) k_rows_light(RowsArgs a)
-{
-    for (int64_t xi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; xi < a.n;
-         xi += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t x = (int32_t)xi;
-        const int dx = a.deg[x];
-        if (dx >= a.light) continue;
-        const int64_t a0 = a.off[x], a1 = a.off[x + 1];
-        double pvacc = 0.0;
-        for (int64_t i = a0; i < a1; ++i) {
-            const int32_t y = a.nb[i];
-            const int dy = a.deg[y];
-            const int64_t dxy = (int64_t)dx * (int64_t)dy;
-            const int64_t b0 = a.off[y], b1 = a.off[y + 1];
-            const int32_t ty = rs_table(a.rs, y);  // x is light: its row is the one walked
-            // common neighbours of x's range [s0, a1) and y's row, ascending: f(z)
-            auto each = [&](int64_t s0, auto&& f) {
-                if (ty >= 0) {
-                    for (int64_t p = s0; p < a1; ++p) {
-                        const int32_t z = a.nb[p];
-                        if (rs_member(a.rs, ty, z)) f(z);
-                    }
-                } else {
-                    intersect_rows(a.nb, s0, a1, b0, b1, a.gallop, [&](int32_t z, int64_t, int64_t) { f(z); });
-                }
-            };
-            if (owns_heavy(a, x, y, dx, dy)) {
-                double peacc = 0.0;
-                each(a0, [&](int32_t z) {
-                    const double w = 1.0 / (double)(dxy * (int64_t)a.deg[z]);
-                    peacc += w;
-                    if (z > y) pvacc += w;
-                });
-                a.pe[i] = peacc;
-            } else {
-                each(i + 1, [&](int32_t z) { pvacc += 1.0 / (double)(dxy * (int64_t)a.deg[z]); });
-            }
+    for (int64_t x = a.x0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < a.x1;
+         x += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q0 = a.off[x], q1 = a.off[x + 1];
+        int64_t e = a.lpos[q0];
+        if (a.lpos[q1] - e >= a.warp_min) continue;  // k_vfold_warp
+        const int64_t dx = a.deg[x];
+        double acc = 0.0;
+        for (int64_t p = q0; p < q1; ++p) {
+            const int64_t e1 = a.lpos[p + 1];
+            if (e1 == e) continue;
+            const int64_t dxy = dx * (int64_t)a.deg[a.nb[p]];
+            for (; e < e1; ++e) acc += 1.0 / (double)(dxy * (int64_t)a.deg[a.lists[e - a.e0]]);
         }
-        a.pv[x] = pvacc;
+        a.pv[x] = acc;
     }
 }
 
-__global__ void __launch_bounds__(kMediumBlock) k_rows_medium(RowsArgs a)
+// Vertices of at least warp_min terms, big[] in descending term count, dealt
+// to warps by an atomic counter.  A warp takes 32 slots at a time: lane j holds
+// slot j's term count, an inclusive scan across lanes gives each term of the
+// group its slot (a five-step search over the lanes), the lanes compute 32
+// weights at once and the warp adds them in lane order.
+__global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int32_t* __restrict__ big,
+                                                            int64_t nbig, unsigned long long* __restrict__ next)
 {
-    __shared__ double s_w[kMediumBlock / 32][32];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int64_t nwarps = (int64_t)gridDim.x * (kMediumBlock / 32);
-    for (int64_t xi = (int64_t)blockIdx.x * (kMediumBlock / 32) + wib; xi < a.n; xi += nwarps) {
-        const int32_t x = (int32_t)xi;
-        const int dx = a.deg[x];
-        if (dx < a.light || dx >= a.hub) continue;  // uniform across the warp
-        const int64_t a0 = a.off[x], a1 = a.off[x + 1];
-        double pvacc = 0.0;
-        for (int64_t i = a0; i < a1; ++i) {
-            const int32_t y = a.nb[i];
-            const int dy = a.deg[y];
-            const int64_t dxy = (int64_t)dx * (int64_t)dy;
-            const bool owner = owns_heavy(a, x, y, dx, dy);
-            const int64_t A0 = owner ? a0 : i + 1, A1 = a1;
-            int64_t B0 = a.off[y];
-            const int64_t B1 = a.off[y + 1];
-            if (!owner && B1 - B0 <= A1 - A0) B0 = lower_bound_row(a.nb, B0, B1, y + 1);  // A holds only z > y
-            double peacc = 0.0;
-            auto chunk = [&](bool hit, int32_t z) {
-                const double w = hit ? 1.0 / (double)(dxy * (int64_t)a.deg[z]) : 0.0;
-                const int below = owner ? __popc(__ballot_sync(0xffffffffu, hit && z < y)) : 0;
-                fold_hits(hit, w, s_w[wib], lane, owner ? &peacc : nullptr, &pvacc, below);
-            };
-            if (A1 - A0 <= B1 - B0) warp_hits(a, A0, A1, y, B0, B1, lane, chunk);
-            else warp_hits(a, B0, B1, x, A0, A1, lane, chunk);
-            if (owner && lane == 0) a.pe[i] = peacc;
-        }
-        if (lane == 0) a.pv[x] = pvacc;
-    }
-}
-
-// Hubs: hubs[] in descending degree.  Warp 0 of the block folds perVertex;
-// warps 1..kHubWarps-1 produce: round r gives them the next kHubWarps-1
-// consecutive y, each writing its y's z > y weights in order to its own region
-// of buffer set r&1 (buf holds 2 x (kHubWarps-1) regions of cap doubles per
-// block; cap >= the largest hub degree bounds the hits of one y), while warp 0
-// folds round r-1 from the other set.  One block barrier per round.
-__global__ void __launch_bounds__(kHubBlock, 2) k_rows_hub(RowsArgs a, const int32_t* __restrict__ hubs,
-                                                            int64_t nhub, double* __restrict__ buf, int64_t cap)
-{
-    constexpr int P = kHubWarps - 1;  // producer warps
-    __shared__ double s_w[kHubWarps][32];
-    __shared__ int64_t s_len[2][P];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    auto region = [&](int set, int w) { return buf + (((int64_t)blockIdx.x * 2 + set) * P + w) * cap; };
-    for (int64_t h = blockIdx.x; h < nhub; h += gridDim.x) {
-        const int32_t x = hubs[h];
-        const int dx = a.deg[x];
-        const int64_t a0 = a.off[x], a1 = a.off[x + 1], d = a1 - a0;
-        // producer warp w (1..P) on slot i: y's z > y weights into region(set, w-1)
-        auto produce = [&](int64_t i, int set) {
-            int64_t len = 0;
-            double* reg = region(set, wib - 1);
-            if (i < a1) {  // uniform across the warp
-                const int32_t y = a.nb[i];
-                const int dy = a.deg[y];
-                const int64_t dxy = (int64_t)dx * (int64_t)dy;
-                const bool owner = owns_heavy(a, x, y, dx, dy);
-                const int64_t A0 = owner ? a0 : i + 1, A1 = a1;
-                int64_t B0 = a.off[y];
-                const int64_t B1 = a.off[y + 1];
-                double peacc = 0.0;
-                auto chunk = [&](bool hit, int32_t z) {
-                    const unsigned mask = __ballot_sync(0xffffffffu, hit);
-                    const int cnt = __popc(mask);
-                    if (cnt == 0) return;
-                    const double w = hit ? 1.0 / (double)(dxy * (int64_t)a.deg[z]) : 0.0;
-                    const int below = owner ? __popc(__ballot_sync(0xffffffffu, hit && z < y)) : 0;
-                    const int rank = __popc(mask & ((1u << lane) - 1u));
-                    if (owner) fold_hits(hit, w, s_w[wib], lane, &peacc, nullptr, 0);
-                    if (hit && rank >= below) reg[len + rank - below] = w;
-                    len += cnt - below;
-                };
-                if (B1 - B0 <= A1 - A0) {
-                    if (!owner) B0 = lower_bound_row(a.nb, B0, B1, y + 1);  // A holds only z > y
-                    warp_hits(a, B0, B1, x, A0, A1, lane, chunk);
-                } else {
-                    warp_hits(a, A0, A1, y, B0, B1, lane, chunk);
-                }
-                if (owner && lane == 0) a.pe[i] = peacc;
-            }
-            if (lane == 0) s_len[set][wib - 1] = len;
-        };
-        double pvacc = 0.0;  // meaningful in warp 0
-        const int64_t rounds = (d + P - 1) / P;
-        if (wib > 0) produce(a0 + wib - 1, 0);
-        __syncthreads();
-        for (int64_t r = 0; r < rounds; ++r) {
-            const int set = (int)(r & 1);
-            if (wib == 0) {
-                for (int w = 0; w < P; ++w) {
-                    const int64_t L = s_len[set][w];
-                    const double* rg = region(set, w);
-                    double v = lane < L ? rg[lane] : 0.0;
-                    for (int64_t k0 = 0; k0 < L; k0 += 32) {
-                        const double vn = k0 + 32 + lane < L ? rg[k0 + 32 + lane] : 0.0;  // next 32, ahead of the chain
-                        const int c = L - k0 < 32 ? (int)(L - k0) : 32;
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(next, 1ull);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        if ((int64_t)b >= nbig) break;
+        const int64_t x = big[b];
+        if (x < a.x0 || x >= a.x1) continue;  // another window's vertex
+        const int64_t dx = a.deg[x];
+        const int64_t q0 = a.off[x], q1 = a.off[x + 1];
+        double acc = 0.0;
+        for (int64_t g0 = q0; g0 < q1; g0 += 32) {
+            const int64_t p = g0 + lane;
+            const bool valid = p < q1;
+            const int64_t len = valid ? a.lpos[p + 1] - a.lpos[p] : 0;
+            int64_t inc = len;
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const double t = __shfl_sync(0xffffffffu, v, j);
-                            if (j < c) pvacc += t;
-                        }
-                        v = vn;
-                    }
-                }
-            } else if (r + 1 < rounds) {
-                produce(a0 + (r + 1) * P + wib - 1, set ^ 1);
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
             }
-            __syncthreads();
+            const int64_t G = __shfl_sync(0xffffffffu, inc, 31);
+            if (G == 0) continue;
+            const int64_t dxy = (valid && len > 0) ? dx * (int64_t)a.deg[a.nb[p]] : 0;
+            const int64_t base = a.lpos[g0] - a.e0;
+            for (int64_t k0 = 0; k0 < G; k0 += 32) {
+                const int64_t e = k0 + lane;
+                // slot of term e: the number of lanes whose inclusive count is <= e
+                int j = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int64_t c = __shfl_sync(0xffffffffu, inc, j + step - 1);
+                    if (c <= e) j += step;
+                }
+                const int64_t dj = __shfl_sync(0xffffffffu, dxy, j & 31);
+                const double w = e < G ? 1.0 / (double)(dj * (int64_t)a.deg[a.lists[base + e]]) : 0.0;
+                const int c = G - k0 < 32 ? (int)(G - k0) : 32;
+#pragma unroll
+                for (int t = 0; t < 32; ++t) {
+                    const double v = __shfl_sync(0xffffffffu, w, t);
+                    if (t < c) acc += v;
+                }
+            }
         }
-        if (threadIdx.x == 0) a.pv[x] = pvacc;
-        __syncthreads();
+        if (lane == 0) a.pv[x] = acc;
     }
 }
 
-__global__ void k_hub_keys(const int32_t* __restrict__ deg, int64_t n, int hub, uint64_t* __restrict__ keys,
-                           unsigned* __restrict__ nh)
+// Vertices of at least warp_min terms, keyed for a descending sort by term count.
+__global__ void k_big_keys(const int64_t* __restrict__ off, const int64_t* __restrict__ lpos, int64_t n,
+                           int64_t warp_min, uint64_t* __restrict__ keys, unsigned* __restrict__ nbig)
 {
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
-        if (deg[v] >= hub)
-            keys[atomicAdd(nh, 1u)] = ((uint64_t)(0x7fffffff - deg[v]) << 32) | (uint64_t)v;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = lpos[off[v + 1]] - lpos[off[v]];
+        if (t >= warp_min) {
+            const uint64_t tc = t < 0xffffffffll ? (uint64_t)t : 0xffffffffull;
+            keys[atomicAdd(nbig, 1u)] = ((0xffffffffull - tc) << 32) | (uint64_t)v;
+        }
+    }
 }
 
-__global__ void k_hub_ids(const uint64_t* __restrict__ keys, int64_t nh, int32_t* __restrict__ ids)
+__global__ void k_low_ids(const uint64_t* __restrict__ keys, int64_t nk, int32_t* __restrict__ ids)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nh; i += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nk; i += (int64_t)gridDim.x * blockDim.x)
         ids[i] = (int32_t)(keys[i] & 0xffffffffu);
+}
+
+// The largest x1 in (x0, n] whose window [x0, x1) holds at most `limit` list
+// entries (x0 + 1 when vertex x0 alone holds more: the caller reports that).
+__global__ void k_window_end(const int64_t* __restrict__ off, const int64_t* __restrict__ lpos, int64_t n, int64_t x0,
+                             int64_t limit, int64_t* __restrict__ out)
+{
+    const int64_t base = lpos[off[x0]];
+    int64_t lo = x0 + 1, hi = n;  // answer in [lo, hi]
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (lpos[off[mid]] - base <= limit) lo = mid;
+        else hi = mid - 1;
+    }
+    *out = lo;
 }
 
 // Row sets: the vertices of at least min_deg neighbours, numbered in id order
@@ -360,93 +344,138 @@ int build_row_sets(rtr_graph* g, Scratch& sc, int min_deg, RowSets* out)
     return RTR_OK;
 }
 
-// perVertex (all vertices) and heavy-edge perEdge from the rows; the caller has
-// run the edge fold and heavy-edge count.  Synchronises the graph's stream.
-int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs)
+// perVertex of every vertex from per-slot lists; the caller has run the edge
+// pass (support, total, perEdge of all edges, cgt).  Synchronises the graph's
+// stream.
+int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt, int64_t* lpos,
+               const int32_t* heavy_list, const unsigned* nheavy)
 {
     cudaStream_t s = g->stream;
-    const int64_t n = g->n;
-    RowsArgs a{g->offsets, g->nbors, g->deg, n, g->pe, g->pv, g->tune_gallop, g->tune_edge, g->tune_heavy,
-               g->count_hub, rs};
-    if (a.hub < a.light) a.hub = a.light;
+    const int64_t n = g->n, m2 = g->m2, m = g->m;
+    if (!cgt) {
+        set_error("rows layout without per-slot term counts (count mode 1 keeps the lists)");
+        return RTR_ERR_STATE;
+    }
+    int64_t* tmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(m2 + 1));
     uint64_t* keys = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
     uint64_t* alt = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
-    unsigned* d_nh = (unsigned*)sc.get(sizeof(unsigned) * 2);
-    if (!keys || !alt || !d_nh) {
-        set_error("device allocation failed (hub list)");
+    unsigned* d_nbig = (unsigned*)sc.get(sizeof(unsigned) * 2);
+    unsigned long long* next = (unsigned long long*)sc.get(sizeof(unsigned long long) * 2);
+    int64_t* d_x1 = (int64_t*)sc.get(sizeof(int64_t) * 2);
+    if (!tmp || !keys || !alt || !d_nbig || !next || !d_x1) {
+        set_error("device allocation failed (rows layout)");
         return RTR_ERR_CUDA;
     }
-    RTR_CUDA_TRY(cudaMemsetAsync(d_nh, 0, sizeof(unsigned), s));
-    k_hub_keys<<<grid_for(n, 256), 256, 0, s>>>(g->deg, n, a.hub, keys, d_nh);
-    unsigned nh = 0;
-    RTR_CUDA_TRY(cudaMemcpyAsync(&nh, d_nh, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    exclusive_scan_i64(cgt, lpos, m2 + 1, nullptr, tmp, s);
+    const int64_t warp_min = g->count_hub;
+    RTR_CUDA_TRY(cudaMemsetAsync(d_nbig, 0, sizeof(unsigned), s));
+    k_big_keys<<<grid_for(n, 256), 256, 0, s>>>(g->offsets, lpos, n, warp_min, keys, d_nbig);
+    int64_t want = 0;
+    unsigned nbig = 0;
+    RTR_CUDA_TRY(cudaMemcpyAsync(&want, lpos + m2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaMemcpyAsync(&nbig, d_nbig, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     RTR_CUDA_TRY(cudaStreamSynchronize(s));
-    g->launches += 1;
-    int32_t* hubs = nullptr;
-    double* hbuf = nullptr;
-    int64_t cap = 0;
-    int hub_grid = 0;
-    if (nh > 0) {
-        void* rtmp = sc.get(radix_temp_bytes(nh));
-        hubs = (int32_t*)sc.get(sizeof(int32_t) * (nh + 1));
-        if (!rtmp || !hubs) {
-            set_error("device allocation failed (hub list)");
-            return RTR_ERR_CUDA;
-        }
-        uint64_t* sorted = radix_sort_u64(keys, alt, nh, 64, rtmp, s);
-        uint64_t first = 0;
-        RTR_CUDA_TRY(cudaMemcpyAsync(&first, sorted, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        k_hub_ids<<<grid_for(nh, 256), 256, 0, s>>>(sorted, nh, hubs);
-        RTR_CUDA_TRY(cudaStreamSynchronize(s));
-        g->launches += 1 + 3 * 8;
-        cap = (int64_t)(0x7fffffff - (int64_t)(first >> 32));  // the largest hub degree
-        int dev_sms = 148;
-        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, g->device);
-        const int64_t want = 2ll * dev_sms;  // two hub blocks per SM
-        hub_grid = (int)((int64_t)nh < want ? (int64_t)nh : want);
-        hbuf = (double*)sc.get(sizeof(double) * (size_t)hub_grid * 2 * (kHubWarps - 1) * (size_t)(cap + 32));
-        if (!hbuf) {
-            set_error("device allocation failed (hub fold buffers, %lld hubs of degree up to %lld)", (long long)nh,
-                      (long long)cap);
-            return RTR_ERR_CUDA;
-        }
-        cap += 32;
-    }
-    cudaEvent_t ready = nullptr, joined = nullptr;
-    if (hub_grid > 0) {
-        if (!g->side) RTR_CUDA_TRY(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking));
-        RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-        RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
-        RTR_CUDA_TRY(cudaEventRecord(ready, s));
-        RTR_CUDA_TRY(cudaStreamWaitEvent(g->side, ready, 0));
-        ktime_begin(g, KT_ROWS_HUB, g->side);
-        k_rows_hub<<<hub_grid, kHubBlock, 0, g->side>>>(a, hubs, nh, hbuf, cap);
-        ktime_end(g, KT_ROWS_HUB, g->side);
-        RTR_CUDA_TRY(cudaEventRecord(joined, g->side));
-        g->launches += 1;
-    }
-    ktime_begin(g, KT_ROWS_LIGHT);
-    k_rows_light<<<grid_for(n, kLightBlock), kLightBlock, 0, s>>>(a);
-    ktime_end(g, KT_ROWS_LIGHT);
-    ktime_begin(g, KT_ROWS_MEDIUM);
-    k_rows_medium<<<grid_for(1ll << 40, kMediumBlock, 16), kMediumBlock, 0, s>>>(a);
-    ktime_end(g, KT_ROWS_MEDIUM);
     g->launches += 2;
-    cudaError_t e = cudaGetLastError();
-    if (joined) {
-        cudaStreamWaitEvent(s, joined, 0);
-        cudaStreamSynchronize(s);  // scratch (hub list, buffers) is freed on return
-        cudaEventDestroy(ready);
-        cudaEventDestroy(joined);
-        ktime_read(g, KT_ROWS_HUB);
-    } else {
-        g->kms[KT_ROWS_HUB] = 0;
+    int32_t* big = nullptr;
+    if (nbig > 0) {
+        void* rtmp = sc.get(radix_temp_bytes(nbig));
+        big = (int32_t*)sc.get(sizeof(int32_t) * (nbig + 1));
+        if (!rtmp || !big) {
+            set_error("device allocation failed (rows layout)");
+            return RTR_ERR_CUDA;
+        }
+        uint64_t* sorted = radix_sort_u64(keys, alt, nbig, 64, rtmp, s);
+        k_low_ids<<<grid_for(nbig, 256), 256, 0, s>>>(sorted, nbig, big);
+        g->launches += 1 + 3 * 8;
     }
-    cudaStreamSynchronize(s);
-    ktime_read(g, KT_ROWS_LIGHT);
-    ktime_read(g, KT_ROWS_MEDIUM);
-    if (e != cudaSuccess) return cuda_fail(e, "rows-layout counting launch", __FILE__, __LINE__);
-    return RTR_OK;
+    // the lists: all of them when they fit in the free HBM (less 1 GiB), else windows of whole rows
+    size_t free_b = 0, total_b = 0;
+    RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const int64_t margin = 1ll << 30;
+    const int64_t fit = (int64_t)free_b > margin ? ((int64_t)free_b - margin) / (int64_t)sizeof(int32_t) : 0;
+    const int64_t room = want < fit ? want : fit;
+    int32_t* lists = (int32_t*)sc.get(sizeof(int32_t) * (room + 1));
+    if (!lists) {
+        set_error("device allocation failed (rows layout: %lld list entries)", (long long)(room + 1));
+        return RTR_ERR_CUDA;
+    }
+    if (!g->side) RTR_CUDA_TRY(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking));
+    cudaEvent_t ready = nullptr, joined = nullptr;
+    RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
+    float ms_fill = 0, ms_fold = 0, ms_warp = 0;
+    int rc = RTR_OK;
+    for (int64_t x0 = 0; x0 < n && rc == RTR_OK;) {
+        int64_t x1 = n;
+        if (want > room) {
+            k_window_end<<<1, 1, 0, s>>>(g->offsets, lpos, n, x0, room, d_x1);
+            g->launches += 1;
+            if (cudaMemcpyAsync(&x1, d_x1, sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = cuda_fail(cudaGetLastError(), "rows-layout window", __FILE__, __LINE__);
+                break;
+            }
+        }
+        int64_t p01[2] = {0, 0}, e01[2] = {0, 0};
+        if (cudaMemcpyAsync(&p01[0], g->offsets + x0, sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(&p01[1], g->offsets + x1, sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess ||
+            cudaMemcpyAsync(&e01[0], lpos + p01[0], sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(&e01[1], lpos + p01[1], sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = cuda_fail(cudaGetLastError(), "rows-layout window", __FILE__, __LINE__);
+            break;
+        }
+        if (e01[1] - e01[0] > room) {
+            set_error("rows layout: vertex %lld alone has %lld perVertex terms, more than the %lld list entries "
+                      "that fit in free device memory",
+                      (long long)x0, (long long)(e01[1] - e01[0]), (long long)room);
+            rc = RTR_ERR_LIMIT;
+            break;
+        }
+        FillArgs fa{g->offsets, g->nbors, g->esrc, g->partner, g->deg, g->fwd, m, g->tune_edge, g->tune_gallop,
+                    rs, lpos, p01[0], p01[1], e01[0], lists};
+        ktime_begin(g, KT_TRI_FILL);
+        k_fill_light<<<grid_for(m, kFillBlock), kFillBlock, 0, s>>>(fa);
+        k_fill_heavy<<<grid_for(1ll << 40, kHeavyBlock, 16), kHeavyBlock, 0, s>>>(fa, heavy_list, nheavy);
+        ktime_end(g, KT_TRI_FILL);
+        FoldArgs fo{g->offsets, g->nbors, g->deg, lpos, e01[0], lists, g->pv, x0, x1, warp_min};
+        cudaMemsetAsync(next, 0, sizeof(unsigned long long), s);
+        ktime_begin(g, KT_VERTEX_FOLD);
+        cudaEventRecord(ready, s);
+        cudaStreamWaitEvent(g->side, ready, 0);
+        ktime_begin(g, KT_FOLD_WARP, g->side);
+        if (nbig > 0) k_vfold_warp<<<grid_for(1ll << 40, kFoldBlock, 8), kFoldBlock, 0, g->side>>>(fo, big, nbig, next);
+        ktime_end(g, KT_FOLD_WARP, g->side);
+        cudaEventRecord(joined, g->side);
+        k_vfold_thread<<<grid_for(x1 - x0, kFoldBlock), kFoldBlock, 0, s>>>(fo);
+        cudaStreamWaitEvent(s, joined, 0);
+        ktime_end(g, KT_VERTEX_FOLD);
+        g->launches += nbig > 0 ? 4 : 3;
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "rows-layout fill / fold launch", __FILE__, __LINE__);
+            break;
+        }
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            rc = cuda_fail(cudaGetLastError(), "rows-layout fill / fold", __FILE__, __LINE__);
+            break;
+        }
+        ktime_read(g, KT_TRI_FILL);
+        ktime_read(g, KT_VERTEX_FOLD);
+        ktime_read(g, KT_FOLD_WARP);
+        ms_fill += g->kms[KT_TRI_FILL];
+        ms_fold += g->kms[KT_VERTEX_FOLD];
+        ms_warp += g->kms[KT_FOLD_WARP];
+        x0 = x1;
+    }
+    cudaStreamSynchronize(g->side);  // scratch is freed on return
+    cudaEventDestroy(ready);
+    cudaEventDestroy(joined);
+    g->kms[KT_TRI_FILL] = ms_fill;
+    g->kms[KT_VERTEX_FOLD] = ms_fold;
+    g->kms[KT_FOLD_WARP] = ms_warp;
+    return rc;
 }
 
 }  // namespace rtr

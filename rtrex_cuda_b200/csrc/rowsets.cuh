@@ -11,6 +11,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "intersect.cuh"
+
 namespace rtr {
 
 // rows of at least this many entries get a hash set
@@ -60,6 +62,60 @@ __device__ __forceinline__ void warp_scan(const int32_t* __restrict__ nb, int64_
         if (__all_sync(0xffffffffu, x > zmax)) break;
         const bool hit = valid && x <= zmax && pred(x);
         chunk(hit, x);
+    }
+}
+
+// Common neighbours z >= from of the rows of a and b, ascending: f(z).  One
+// thread.  The shorter row is walked and its elements looked up in the longer
+// row's hash set when that row has one; otherwise the rows merge or gallop
+// (intersect_rows).  from = INT32_MIN visits every common neighbour.
+template <typename F>
+__device__ __forceinline__ void thread_common(const RowSets& rs, const int64_t* __restrict__ off,
+                                              const int32_t* __restrict__ nb, int32_t a, int32_t b, int32_t from,
+                                              int gallop, F&& f)
+{
+    int64_t a0 = off[a], a1 = off[a + 1], b0 = off[b], b1 = off[b + 1];
+    if (a0 == a1 || b0 == b1) return;
+    const bool a_short = a1 - a0 <= b1 - b0;
+    const int32_t t = rs_table(rs, a_short ? b : a);
+    const bool cut = from != INT32_MIN;
+    if (t >= 0) {
+        int64_t s0 = a_short ? a0 : b0;
+        const int64_t s1 = a_short ? a1 : b1;
+        if (cut) s0 = lower_bound_row(nb, s0, s1, from);
+        const int32_t zmax = nb[(a_short ? b1 : a1) - 1];
+        for (int64_t p = s0; p < s1; ++p) {
+            const int32_t z = nb[p];
+            if (z > zmax) break;
+            if (rs_member(rs, t, z)) f(z);
+        }
+        return;
+    }
+    if (cut) {
+        a0 = lower_bound_row(nb, a0, a1, from);
+        b0 = lower_bound_row(nb, b0, b1, from);
+    }
+    intersect_rows(nb, a0, a1, b0, b1, gallop, [&](int32_t z, int64_t, int64_t) { f(z); });
+}
+
+// The warp's hits of the ascending range S = [s0, s1) in the row of w, whose
+// range is [l0, l1): chunk(hit, z) per 32 elements of S (every lane, warp-
+// uniform control flow), hits ascending.  Through w's hash set when it has one
+// (the caller passes w's whole row, or a part of it holding every element of S
+// that is in the row), else by binary search in [l0, l1).
+template <typename F>
+__device__ __forceinline__ void warp_walk(const RowSets& rs, const int64_t* __restrict__ off,
+                                          const int32_t* __restrict__ nb, int64_t s0, int64_t s1, int32_t w,
+                                          int64_t l0, int64_t l1, int lane, F&& chunk)
+{
+    if (s0 >= s1 || l0 >= l1) return;
+    const int32_t t = rs_table(rs, w);
+    if (t >= 0) {
+        const int32_t zmax = nb[off[w + 1] - 1];
+        warp_scan(nb, s0, s1, zmax, lane, [&](int32_t z) { return rs_member(rs, t, z); }, chunk);
+    } else {
+        warp_chunks(nb, s0, s1, l0, l1, lane,
+                    [&](int64_t lo, int64_t hi, int32_t v) { return lower_bound_row(nb, lo, hi, v); }, chunk);
     }
 }
 

@@ -84,9 +84,9 @@ struct rtr_graph {
     int tune_edge = 1024;  // deg u + deg v from which an edge is intersected by a warp
     // counting layout: 0 keep triangle lists when they fit in free device memory,
     // 1 always keep them, 2 never (rows layout: folds straight from the CSR);
-    // count_hub: degree from which the rows layout gives a vertex a thread block
+    // count_hub: perVertex terms from which the rows layout folds a vertex with a warp
     int count_mode = 0;
-    int count_hub = 4096;
+    int count_hub = 1024;
     bool lists = false;  // the last count kept the triangle lists (the clean needs them)
     // clean units with at least this many seeds and triangle lists of at most
     // this mean length replay in parallel rounds (one thread block each); the
@@ -106,8 +106,8 @@ struct rtr_graph {
     float ms_build = 0, ms_count = 0, ms_clean = 0, ms_extract = 0, ms_decompose = 0, ms_expand = 0;
     // per-kernel device times of the last run (ms), CUDA events on the graph's stream:
     // [0] k_edge_fold [1] k_tri_fill [2] k_vertex_fold [3] k_clean_units [4] k_extract_components
-    // [5] decompose [6] k_rows_light [7] k_rows_medium [8] k_rows_hub (rows layout; the hub
-    // kernel on the second stream, concurrent with the other two)
+    // [5] decompose [6] k_edge_fold alone [7] k_edge_count_heavy alone [8] the rows
+    // layout's warp perVertex fold (second stream, concurrent with the thread fold)
     static constexpr int kTimers = 10;
     cudaEvent_t kev[2 * kTimers] = {};
     float kms[kTimers] = {};
@@ -137,9 +137,9 @@ enum KernelTimer {
     KT_CLEAN_UNITS,
     KT_EXTRACT,
     KT_DECOMPOSE,
-    KT_ROWS_LIGHT,
-    KT_ROWS_MEDIUM,
-    KT_ROWS_HUB
+    KT_EDGE_LIGHT,
+    KT_EDGE_HEAVY,
+    KT_FOLD_WARP
 };
 inline void ktime_begin(rtr_graph* g, int k, cudaStream_t s = nullptr)
 {
@@ -172,8 +172,10 @@ int count_triangles(rtr_graph* g);
 struct RowSets;
 // hash sets of the rows of at least min_deg entries, in sc (count_rows.cu)
 int build_row_sets(rtr_graph* g, Scratch& sc, int min_deg, RowSets* out);
-// list-free perVertex / heavy perEdge (count_rows.cu)
-int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs);
+// rows layout: perVertex from per-slot lists of z (count_rows.cu); cgt the
+// per-slot term counts, lpos room for their scan, heavy_list the heavy edges
+int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt, int64_t* lpos,
+               const int32_t* heavy_list, const unsigned* nheavy);
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 int initial_clean(rtr_graph* g, double eps);
 int extract_clusters(rtr_graph* g);

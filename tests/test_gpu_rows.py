@@ -1,9 +1,10 @@
-"""Counting in the rows layout (no triangle lists): perVertex and heavy-edge
-perEdge folded straight from the CSR rows (rtrex_cuda_b200/csrc/count_rows.cu).
+"""Counting in the rows layout (no triangle lists): perEdge from the edge pass,
+perVertex folded from 4-byte per-slot lists of its z > y terms
+(rtrex_cuda_b200/csrc/count_rows.cu).
 
 * Every fixture case, with work splits that send every vertex through each of
-  the three kernels (thread, warp, thread block) and every edge through the
-  heavy-edge path, bit for bit against the oracle's commonNbr restatement.
+  the two perVertex folds (thread, warp) and every edge through the heavy-edge
+  (warp) fill, bit for bit against the oracle's commonNbr restatement.
 * The device R-MAT generator against its numpy definition.
 * R-MAT scale 22 (2.1 G triangles: its lists would need ~200 GB, so the
   default count mode picks the rows layout by itself): the exact total against
@@ -21,15 +22,15 @@ from tests import helpers
 
 pytestmark = pytest.mark.gpu
 
-# (gallop, light degree, heavy-edge degree sum, hub degree): the default split,
-# then splits that push every vertex to one kernel and every edge to the
-# rows path's heavy-edge fold
+# (gallop, light degree, heavy-edge degree sum, perVertex terms from which a
+# warp folds): the default split, then splits that push every vertex to one
+# fold and every edge to the warp path
 SPLITS = [
-    (16, 32, 1024, 4096),
-    (16, 1 << 30, 1024, 1 << 30),  # thread per vertex
-    (4, 1, 1, 1 << 30),            # warp per vertex, every edge heavy
-    (16, 1, 1, 1),                 # thread block per vertex, every edge heavy
-    (64, 4, 8, 16),                # a mix
+    (16, 32, 1024, 1024),
+    (16, 1 << 30, 1 << 30, 1 << 30),  # every edge a thread, every vertex a thread
+    (4, 1, 1, 1 << 30),               # every edge a warp, every vertex a thread
+    (16, 1, 1, 1),                    # every edge a warp, every vertex with terms a warp
+    (64, 4, 8, 16),                   # a mix
 ]
 
 
