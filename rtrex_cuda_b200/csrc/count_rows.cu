@@ -187,7 +187,17 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
             if (G == 0) continue;
             const int64_t dxy = (valid && len > 0) ? dx * (int64_t)a.deg[a.nb[p]] : 0;
             const int64_t base = a.lpos[g0] - a.e0;
+            // the lanes' terms four chunks ahead and their degrees one chunk ahead of the add chain
+            auto zload = [&](int64_t k0) -> int32_t {
+                const int64_t e = k0 + lane;
+                return e < G ? __ldg(a.lists + base + e) : -1;
+            };
+            int32_t z1 = zload(32), z2 = zload(64), z3 = zload(96);
+            const int32_t z0 = zload(0);
+            int64_t dz = z0 >= 0 ? a.deg[z0] : 1;
             for (int64_t k0 = 0; k0 < G; k0 += 32) {
+                const int32_t z4 = zload(k0 + 128);
+                const int64_t dzn = z1 >= 0 ? a.deg[z1] : 1;
                 const int64_t e = k0 + lane;
                 // slot of term e: the number of lanes whose inclusive count is <= e
                 int j = 0;
@@ -197,13 +207,17 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
                     if (c <= e) j += step;
                 }
                 const int64_t dj = __shfl_sync(0xffffffffu, dxy, j & 31);
-                const double w = e < G ? 1.0 / (double)(dj * (int64_t)a.deg[a.lists[base + e]]) : 0.0;
+                const double w = e < G ? 1.0 / (double)(dj * dz) : 0.0;
                 const int c = G - k0 < 32 ? (int)(G - k0) : 32;
 #pragma unroll
                 for (int t = 0; t < 32; ++t) {
                     const double v = __shfl_sync(0xffffffffu, w, t);
                     if (t < c) acc += v;
                 }
+                z1 = z2;
+                z2 = z3;
+                z3 = z4;
+                dz = dzn;
             }
         }
         if (lane == 0) a.pv[x] = acc;
@@ -245,7 +259,8 @@ __global__ void k_window_end(const int64_t* __restrict__ off, const int64_t* __r
 }
 
 // Row sets: the vertices of at least min_deg neighbours, numbered in id order
-// (flag + scan), each with a power-of-two table of >= 2 deg slots.
+// (flag + scan), each with a power-of-two number of 8-key buckets, >= 4 slots
+// per key.
 __global__ void k_rs_flags(const int32_t* __restrict__ deg, int64_t n, int min_deg, int64_t* __restrict__ flag)
 {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v <= n; v += (int64_t)gridDim.x * blockDim.x)
@@ -262,17 +277,18 @@ __global__ void k_rs_sizes(const int32_t* __restrict__ deg, int64_t n, const int
             continue;
         }
         const int32_t t = (int32_t)num[v];
-        int bits = 1;
-        while ((1ll << bits) < 2ll * deg[v]) ++bits;
+        int bits = 0;
+        while ((int64_t)kBucketKeys << bits < 4ll * deg[v]) ++bits;
         tab[v] = t;
         owner[t] = (int32_t)v;
         tbits[t] = bits;
-        tsize[t] = 1ll << bits;
+        tsize[t] = (int64_t)kBucketKeys << bits;
     }
 }
 
-// A warp per table (dealt modulo the warp count) inserts its row; the table
-// is at least half empty, so every probe sequence meets an empty slot.
+// A warp per table (dealt modulo the warp count) inserts its row: each key
+// takes the first empty slot of the first bucket, from its own, that has one
+// (the table is at most a quarter full, so every key finds one).
 __global__ void k_rs_insert(const int32_t* __restrict__ owner, int64_t nt, const int64_t* __restrict__ off,
                             const int32_t* __restrict__ nb, const int64_t* __restrict__ toff,
                             const int32_t* __restrict__ tbits, int32_t* __restrict__ slot)
@@ -286,8 +302,10 @@ __global__ void k_rs_insert(const int32_t* __restrict__ owner, int64_t nt, const
         int32_t* tb = slot + toff[t];
         for (int64_t p = off[v] + lane; p < off[v + 1]; p += 32) {
             const int32_t z = nb[p];
-            uint32_t h = rs_hash(z, bits);
-            while (atomicCAS(&tb[h], -1, z) != -1) h = (h + 1u) & mask;
+            bool placed = false;
+            for (uint32_t b = rs_hash(z, bits); !placed; b = (b + 1u) & mask)
+                for (int k = 0; k < kBucketKeys && !placed; ++k)
+                    placed = atomicCAS(&tb[(int64_t)b * kBucketKeys + k], -1, z) == -1;
         }
     }
 }

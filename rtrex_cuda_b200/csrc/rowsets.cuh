@@ -1,11 +1,12 @@
-// Hash sets of long CSR rows, for membership lookups that cost one or two
-// independent loads instead of a binary search's chain of dependent ones.
-// Built by build_row_sets (count_rows.cu) for every vertex of at least a given
-// degree: open addressing with linear probing over a power-of-two table of at
-// least twice the row's length (so every probe sequence ends), keys the
-// neighbour ids, -1 empty.  Rows hold distinct ids, so a set answers exactly
-// "is z a neighbour of w"; the counting folds only need that (the weight of a
-// common neighbour z depends on z alone), not z's slot.
+// Hash sets of long CSR rows, for membership lookups that cost about one
+// memory transaction instead of a binary search's chain of dependent loads.
+// Built by build_row_sets (count_rows.cu) for every vertex of at least
+// kSetDegree neighbours: buckets of 8 keys (one 32-byte sector), a power-of-two
+// number of them with at least 4 slots per key, linear probing over buckets;
+// -1 marks an empty slot and a bucket's keys fill its slots from the first, so
+// a lookup ends at the first bucket that still has an empty slot.  Rows hold
+// distinct ids, so a set answers exactly "is z a neighbour of w"; the counting
+// folds only need that (the weight of a common neighbour z depends on z alone).
 #pragma once
 
 #include <cstdint>
@@ -17,11 +18,12 @@ namespace rtr {
 
 // rows of at least this many entries get a hash set
 constexpr int kSetDegree = 256;
+constexpr int kBucketKeys = 8;
 
 struct RowSets {
     const int32_t* tab;    // vertex -> its table, -1 for rows without one (null: no tables at all)
-    const int64_t* toff;   // table -> first slot
-    const int32_t* tbits;  // table -> log2 of its slot count
+    const int64_t* toff;   // table -> first slot (a multiple of kBucketKeys)
+    const int32_t* tbits;  // table -> log2 of its bucket count
     const int32_t* slot;   // the keys, -1 for empty slots
 };
 
@@ -29,20 +31,21 @@ __device__ __forceinline__ int32_t rs_table(const RowSets& r, int32_t w) { retur
 
 __device__ __forceinline__ uint32_t rs_hash(int32_t z, int bits)
 {
-    return ((uint32_t)z * 2654435761u) >> (32 - bits);
+    return bits == 0 ? 0u : ((uint32_t)z * 2654435761u) >> (32 - bits);
 }
 
 __device__ __forceinline__ bool rs_member(const RowSets& r, int32_t t, int32_t z)
 {
-    const int64_t base = r.toff[t];
+    const int4* tb = reinterpret_cast<const int4*>(r.slot + r.toff[t]);
     const int bits = r.tbits[t];
     const uint32_t mask = (1u << bits) - 1u;
-    uint32_t h = rs_hash(z, bits);
+    uint32_t b = rs_hash(z, bits);
     while (true) {
-        const int32_t k = r.slot[base + h];
-        if (k == z) return true;
-        if (k < 0) return false;
-        h = (h + 1u) & mask;
+        const int4 k0 = __ldg(tb + 2 * b), k1 = __ldg(tb + 2 * b + 1);
+        if (k0.x == z || k0.y == z || k0.z == z || k0.w == z || k1.x == z || k1.y == z || k1.z == z || k1.w == z)
+            return true;
+        if (k1.w < 0) return false;  // the bucket is not full: z would be in it
+        b = (b + 1u) & mask;
     }
 }
 
@@ -55,12 +58,13 @@ template <typename Pred, typename F>
 __device__ __forceinline__ void warp_scan(const int32_t* __restrict__ nb, int64_t s0, int64_t s1, int32_t zmax,
                                           int lane, Pred&& pred, F&& chunk)
 {
+    int32_t xn = s0 + lane < s1 ? nb[s0 + lane] : 0x7fffffff;
     for (int64_t base = s0; base < s1; base += 32) {
-        const int64_t p = base + lane;
-        const bool valid = p < s1;
-        const int32_t x = valid ? nb[p] : 0x7fffffff;
+        const int32_t x = xn;
+        const int64_t pn = base + 32 + lane;
+        xn = pn < s1 ? nb[pn] : 0x7fffffff;  // the next chunk, loaded ahead of this one's lookups
         if (__all_sync(0xffffffffu, x > zmax)) break;
-        const bool hit = valid && x <= zmax && pred(x);
+        const bool hit = base + lane < s1 && x <= zmax && pred(x);
         chunk(hit, x);
     }
 }
