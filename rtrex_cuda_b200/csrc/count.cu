@@ -186,6 +186,28 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
     if (lane == 0 && tri) atomicAdd(total, tri);
 }
 
+// Heavy edges keyed by the vertex whose hash set their intersection probes
+// (the longer row; the shorter one is walked): sorted on it, the warps running
+// at any one time probe a few sets, which then stay in L2.
+__global__ void k_heavy_keys(const int64_t* __restrict__ off, const int32_t* __restrict__ esrc,
+                             const int32_t* __restrict__ nb, const int32_t* __restrict__ fwd,
+                             const int32_t* __restrict__ heavy_list, int64_t nh, uint64_t* __restrict__ keys)
+{
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nh; h += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t k = heavy_list[h];
+        const int64_t i = fwd[k];
+        const int32_t u = esrc[i], v = nb[i];
+        const int32_t w = off[u + 1] - off[u] <= off[v + 1] - off[v] ? v : u;
+        keys[h] = ((uint64_t)(uint32_t)k << 32) | (uint64_t)(uint32_t)w;
+    }
+}
+
+__global__ void k_heavy_order(const uint64_t* __restrict__ keys, int64_t nh, int32_t* __restrict__ heavy_list)
+{
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nh; h += (int64_t)gridDim.x * blockDim.x)
+        heavy_list[h] = (int32_t)(keys[h] >> 32);
+}
+
 __global__ void __launch_bounds__(kHeavyEdgeBlock)
     k_tri_fill_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                      const int32_t* __restrict__ deg, const int32_t* __restrict__ partner,
@@ -411,6 +433,26 @@ int count_triangles(rtr_graph* g)
     k_edge_fold<<<ge, kBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, g->partner, m, rs, g->pe,
                                       g->sup, cnt, cgt, g->ctr, g->tune_gallop, g->tune_edge, heavy_list, nheavy);
     ktime_end(g, KT_EDGE_LIGHT);
+    if (rs.tab) {  // heavy edges in the order of the sets they probe
+        unsigned nh = 0;
+        RTR_CUDA_TRY(cudaMemcpyAsync(&nh, nheavy, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        RTR_CUDA_TRY(cudaStreamSynchronize(s));
+        if (nh > 1) {
+            uint64_t* hkeys = (uint64_t*)sc.get(sizeof(uint64_t) * (nh + 1));
+            uint64_t* halt = (uint64_t*)sc.get(sizeof(uint64_t) * (nh + 1));
+            void* htmp = sc.get(radix_temp_bytes(nh));
+            if (!hkeys || !halt || !htmp) {
+                set_error("device allocation failed (heavy-edge order)");
+                return RTR_ERR_CUDA;
+            }
+            k_heavy_keys<<<grid_for(nh, 256), 256, 0, s>>>(g->offsets, g->esrc, g->nbors, g->fwd, heavy_list, nh,
+                                                            hkeys);
+            const uint64_t* sorted = radix_sort_u64(hkeys, halt, nh, bits_for((uint64_t)(n > 0 ? n - 1 : 0)),
+                                                    htmp, s);
+            k_heavy_order<<<grid_for(nh, 256), 256, 0, s>>>(sorted, nh, heavy_list);
+            g->launches += 2 + 3 * ((bits_for((uint64_t)(n > 0 ? n - 1 : 0)) + 7) / 8);
+        }
+    }
     ktime_begin(g, KT_EDGE_HEAVY);
     k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, g->partner,
                                                       heavy_list, nheavy, g->tune_gallop, rs, g->sup, cnt, cgt,

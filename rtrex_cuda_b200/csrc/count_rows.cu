@@ -28,7 +28,8 @@
 //             vertices dealt from a queue in descending term count, the
 //             weights of 32 terms computed by the lanes and added in lane
 //             order (the one sequential part: ~10^8 adds for the largest
-//             R-MAT scale-24 hub).
+//             R-MAT scale-24 hub), with the terms and their degrees loaded
+//             blocks ahead of the add chain.
 // Membership lookups use the hash sets of the long rows (rowsets.cuh,
 // build_row_sets below).
 #include "intersect.cuh"
@@ -187,37 +188,55 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
             if (G == 0) continue;
             const int64_t dxy = (valid && len > 0) ? dx * (int64_t)a.deg[a.nb[p]] : 0;
             const int64_t base = a.lpos[g0] - a.e0;
-            // the lanes' terms four chunks ahead and their degrees one chunk ahead of the add chain
+            // Software pipeline over blocks of 4 chunks (128 terms): the lanes' terms
+            // are loaded two blocks ahead and their degrees one block ahead of the
+            // add chain, so the chain does not wait on either load.
             auto zload = [&](int64_t k0) -> int32_t {
                 const int64_t e = k0 + lane;
                 return e < G ? __ldg(a.lists + base + e) : -1;
             };
-            int32_t z1 = zload(32), z2 = zload(64), z3 = zload(96);
-            const int32_t z0 = zload(0);
-            int64_t dz = z0 >= 0 ? a.deg[z0] : 1;
-            for (int64_t k0 = 0; k0 < G; k0 += 32) {
-                const int32_t z4 = zload(k0 + 128);
-                const int64_t dzn = z1 >= 0 ? a.deg[z1] : 1;
-                const int64_t e = k0 + lane;
-                // slot of term e: the number of lanes whose inclusive count is <= e
-                int j = 0;
+            auto dload = [&](int32_t z) -> int32_t { return z >= 0 ? __ldg(a.deg + z) : 1; };
+            int32_t zA[4], zB[4], dA[4];
 #pragma unroll
-                for (int step = 16; step > 0; step >>= 1) {
-                    const int64_t c = __shfl_sync(0xffffffffu, inc, j + step - 1);
-                    if (c <= e) j += step;
-                }
-                const int64_t dj = __shfl_sync(0xffffffffu, dxy, j & 31);
-                const double w = e < G ? 1.0 / (double)(dj * dz) : 0.0;
-                const int c = G - k0 < 32 ? (int)(G - k0) : 32;
+            for (int c = 0; c < 4; ++c) zA[c] = zload(32 * c);
 #pragma unroll
-                for (int t = 0; t < 32; ++t) {
-                    const double v = __shfl_sync(0xffffffffu, w, t);
-                    if (t < c) acc += v;
+            for (int c = 0; c < 4; ++c) zB[c] = zload(128 + 32 * c);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) dA[c] = dload(zA[c]);
+            for (int64_t b0 = 0; b0 < G; b0 += 128) {
+                int32_t zC[4], dB[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) zC[c] = zload(b0 + 256 + 32 * c);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) dB[c] = dload(zB[c]);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int64_t k0 = b0 + 32 * c;
+                    if (k0 < G) {  // uniform across the warp
+                        const int64_t e = k0 + lane;
+                        // slot of term e: the number of lanes whose inclusive count is <= e
+                        int q = 0;
+#pragma unroll
+                        for (int step = 16; step > 0; step >>= 1) {
+                            const int64_t cq = __shfl_sync(0xffffffffu, inc, q + step - 1);
+                            if (cq <= e) q += step;
+                        }
+                        const int64_t dq = __shfl_sync(0xffffffffu, dxy, q & 31);
+                        const double w = e < G ? 1.0 / (double)(dq * (int64_t)dA[c]) : 0.0;
+                        const int cnt = G - k0 < 32 ? (int)(G - k0) : 32;
+#pragma unroll
+                        for (int t = 0; t < 32; ++t) {
+                            const double v = __shfl_sync(0xffffffffu, w, t);
+                            if (t < cnt) acc += v;
+                        }
+                    }
                 }
-                z1 = z2;
-                z2 = z3;
-                z3 = z4;
-                dz = dzn;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    zA[c] = zB[c];
+                    zB[c] = zC[c];
+                    dA[c] = dB[c];
+                }
             }
         }
         if (lane == 0) a.pv[x] = acc;
@@ -421,7 +440,7 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
     cudaEvent_t ready = nullptr, joined = nullptr;
     RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
     RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
-    float ms_fill = 0, ms_fold = 0, ms_warp = 0;
+    float ms_fill = 0, ms_fold = 0, ms_warp = 0, ms_fill_l = 0, ms_fill_h = 0;
     int rc = RTR_OK;
     for (int64_t x0 = 0; x0 < n && rc == RTR_OK;) {
         int64_t x1 = n;
@@ -454,8 +473,12 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         FillArgs fa{g->offsets, g->nbors, g->esrc, g->partner, g->deg, g->fwd, m, g->tune_edge, g->tune_gallop,
                     rs, lpos, p01[0], p01[1], e01[0], lists};
         ktime_begin(g, KT_TRI_FILL);
+        ktime_begin(g, KT_FILL_LIGHT);
         k_fill_light<<<grid_for(m, kFillBlock), kFillBlock, 0, s>>>(fa);
+        ktime_end(g, KT_FILL_LIGHT);
+        ktime_begin(g, KT_FILL_HEAVY);
         k_fill_heavy<<<grid_for(1ll << 40, kHeavyBlock, 16), kHeavyBlock, 0, s>>>(fa, heavy_list, nheavy);
+        ktime_end(g, KT_FILL_HEAVY);
         ktime_end(g, KT_TRI_FILL);
         FoldArgs fo{g->offsets, g->nbors, g->deg, lpos, e01[0], lists, g->pv, x0, x1, warp_min};
         cudaMemsetAsync(next, 0, sizeof(unsigned long long), s);
@@ -482,6 +505,10 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         ktime_read(g, KT_TRI_FILL);
         ktime_read(g, KT_VERTEX_FOLD);
         ktime_read(g, KT_FOLD_WARP);
+        ktime_read(g, KT_FILL_LIGHT);
+        ktime_read(g, KT_FILL_HEAVY);
+        ms_fill_l += g->kms[KT_FILL_LIGHT];
+        ms_fill_h += g->kms[KT_FILL_HEAVY];
         ms_fill += g->kms[KT_TRI_FILL];
         ms_fold += g->kms[KT_VERTEX_FOLD];
         ms_warp += g->kms[KT_FOLD_WARP];
@@ -493,6 +520,8 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
     g->kms[KT_TRI_FILL] = ms_fill;
     g->kms[KT_VERTEX_FOLD] = ms_fold;
     g->kms[KT_FOLD_WARP] = ms_warp;
+    g->kms[KT_FILL_LIGHT] = ms_fill_l;
+    g->kms[KT_FILL_HEAVY] = ms_fill_h;
     return rc;
 }
 
