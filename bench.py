@@ -353,7 +353,8 @@ def rmat24_leg(args, dev, flush_l2, peak, peak_kind, scale=24, steps=None, mode=
                          "edge_fold_light_edges": kms["k_edge_fold_light"],
                          "edge_count_heavy_edges": kms["k_edge_count_heavy"], "list_fill": kms["k_tri_fill"],
                          "list_fill_light": kms["k_fill_light"], "list_fill_heavy": kms["k_fill_heavy"],
-                         "vertex_fold": kms["k_vertex_fold"], "vertex_fold_warps": kms["k_vfold_warp"]},
+                         "vertex_fold": kms["k_vertex_fold"], "vertex_fold_warps": kms["k_vfold_warp"],
+                         "vertex_fold_blocks": kms["k_vfold_block"]},
            "gpu_launches_per_count": launches,
            "roofline_count": {"bound": "hbm", "algorithmic_bytes": b_count, "oriented_sum": osum,
                               "achieved": b_count / t / 1e9, "peak": peak, "unit": "GB/s",

@@ -331,7 +331,8 @@ class Graph:
                 "launches": int(launches.value), "residual_warnings": int(resid.value)}
 
     KERNELS = ("k_edge_fold", "k_tri_fill", "k_vertex_fold", "k_clean_units", "k_extract_components", "decompose",
-               "k_edge_fold_light", "k_edge_count_heavy", "k_vfold_warp", "k_fill_light", "k_fill_heavy")
+               "k_edge_fold_light", "k_edge_count_heavy", "k_vfold_warp", "k_fill_light", "k_fill_heavy",
+               "k_vfold_block")
 
     def kernel_ms(self) -> dict:
         """Device times (ms) of the last run's main kernels and of the whole decompose."""

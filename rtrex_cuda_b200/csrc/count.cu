@@ -149,20 +149,38 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
         // the shorter row walked against the longer one
         const bool u_short = u1 - u0 <= v1 - v0;
         const int32_t t = rs_table(rs, u_short ? v : u);
-        if (pe || t >= 0) {
-            const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
-            double acc = 0.0;
+        const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
+        double acc = 0.0;
+        if (t >= 0) {
+            // 4 chunks per step, their lookups and then their degrees in flight together
+            constexpr int B = 4;
+            warp_probe_walk<B>(rs, t, nb, u_short ? u0 : v0, u_short ? u1 : v1, nb[(u_short ? v1 : u1) - 1], lane,
+                               [&](const bool (&hit)[B], const int32_t (&x)[B]) {
+                                   int32_t dz[B];
+#pragma unroll
+                                   for (int b = 0; b < B; ++b) dz[b] = (pe && hit[b]) ? deg[x[b]] : 1;
+#pragma unroll
+                                   for (int b = 0; b < B; ++b) {
+                                       c += hit[b] ? 1u : 0u;
+                                       above += (hit[b] && x[b] > v) ? 1u : 0u;
+                                       above_u += (hit[b] && x[b] > u) ? 1u : 0u;
+                                       if (pe) {
+                                           const double w = hit[b] ? 1.0 / (double)(duv * (int64_t)dz[b]) : 0.0;
+                                           fold_hits(hit[b], w, s_w[wib], lane, &acc, nullptr, 0);
+                                       }
+                                   }
+                               });
+            if (pe && lane == 0) pe[i] = acc;
+        } else if (pe) {
             warp_walk(rs, off, nb, u_short ? u0 : v0, u_short ? u1 : v1, u_short ? v : u, u_short ? v0 : u0,
                       u_short ? v1 : u1, lane, [&](bool hit, int32_t z) {
                           c += hit ? 1u : 0u;
                           above += (hit && z > v) ? 1u : 0u;
                           above_u += (hit && z > u) ? 1u : 0u;
-                          if (pe) {
-                              const double w = hit ? 1.0 / (double)(duv * (int64_t)deg[z]) : 0.0;
-                              fold_hits(hit, w, s_w[wib], lane, &acc, nullptr, 0);
-                          }
+                          const double w = hit ? 1.0 / (double)(duv * (int64_t)deg[z]) : 0.0;
+                          fold_hits(hit, w, s_w[wib], lane, &acc, nullptr, 0);
                       });
-            if (pe && lane == 0) pe[i] = acc;
+            if (lane == 0) pe[i] = acc;
         } else {
             warp_intersect_part(nb, u0, u1, v0, v1, gallop, lane, [&](int32_t z, int64_t, int64_t) {
                 ++c;

@@ -105,17 +105,27 @@ __global__ void __launch_bounds__(kHeavyBlock) k_fill_heavy(FillArgs a, const in
         const bool u_short = u1 - u0 <= v1 - v0;
         const int64_t s1 = u_short ? u1 : v1;
         const int64_t s0 = lower_bound_row(a.nb, u_short ? u0 : v0, s1, from);
-        warp_walk(a.rs, a.off, a.nb, s0, s1, u_short ? v : u, u_short ? v0 : u0, u_short ? v1 : u1, lane,
-                  [&](bool hit, int32_t z) {
-                      const bool to_r = hit && wr, to_i = hit && wi && z > v;
-                      const unsigned mr = __ballot_sync(0xffffffffu, to_r);
-                      const unsigned mi = __ballot_sync(0xffffffffu, to_i);
-                      const int64_t wr_at = qr + __popc(mr & lt), wi_at = qi + __popc(mi & lt);
-                      if (to_r && wr_at < qr1) a.lists[wr_at] = z;
-                      if (to_i && wi_at < qi1) a.lists[wi_at] = z;
-                      qr += __popc(mr);
-                      qi += __popc(mi);
-                  });
+        auto emit = [&](bool hit, int32_t z) {
+            const bool to_r = hit && wr, to_i = hit && wi && z > v;
+            const unsigned mr = __ballot_sync(0xffffffffu, to_r);
+            const unsigned mi = __ballot_sync(0xffffffffu, to_i);
+            const int64_t wr_at = qr + __popc(mr & lt), wi_at = qi + __popc(mi & lt);
+            if (to_r && wr_at < qr1) a.lists[wr_at] = z;
+            if (to_i && wi_at < qi1) a.lists[wi_at] = z;
+            qr += __popc(mr);
+            qi += __popc(mi);
+        };
+        const int32_t t = rs_table(a.rs, u_short ? v : u);
+        if (t >= 0) {
+            constexpr int B = 4;  // 4 chunks per step, their lookups in flight together
+            warp_probe_walk<B>(a.rs, t, a.nb, s0, s1, a.nb[(u_short ? v1 : u1) - 1], lane,
+                               [&](const bool (&hit)[B], const int32_t (&x)[B]) {
+#pragma unroll
+                                   for (int b = 0; b < B; ++b) emit(hit[b], x[b]);
+                               });
+        } else {
+            warp_walk(a.rs, a.off, a.nb, s0, s1, u_short ? v : u, u_short ? v0 : u0, u_short ? v1 : u1, lane, emit);
+        }
     }
 }
 
@@ -243,12 +253,111 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
     }
 }
 
+// The largest vertices (at least block_min terms), a thread block each, from
+// the front of big[] (descending term count): warp 0 runs the add chain and
+// nothing else, warps 1..7 produce the weights.  The terms of x are cut into
+// segments of kSeg; round r gives the producers the next 7 segments, each lane
+// loading its 32 terms and their degrees with all loads in flight at once and
+// writing 32 weights to the segment's shared-memory buffer (set r&1), while
+// warp 0 adds the previous round's 7 segments in order.  One block barrier per
+// round; the chain costs one double add per term.
+constexpr int kSeg = 1024;
+constexpr int kSegChunks = kSeg / 32;
+constexpr int kProducers = kFoldBlock / 32 - 1;
+constexpr size_t kBlockFoldSmem = sizeof(double) * 2 * kProducers * kSeg;
+
+__global__ void __launch_bounds__(kFoldBlock) k_vfold_block(FoldArgs a, const int32_t* __restrict__ huge,
+                                                             int64_t nhuge, unsigned long long* __restrict__ next)
+{
+    extern __shared__ double s_buf[];  // [2][kProducers][kSeg]
+    __shared__ int64_t s_x;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned long long b = atomicAdd(next, 1ull);
+            s_x = (int64_t)b < nhuge ? huge[b] : -1;
+        }
+        __syncthreads();
+        const int64_t x = s_x;
+        if (x < 0) break;  // uniform across the block
+        if (x >= a.x0 && x < a.x1) {
+            const int64_t q0 = a.off[x], q1 = a.off[x + 1];
+            const int64_t E0 = a.lpos[q0], T = a.lpos[q1] - E0;
+            const int64_t dx = a.deg[x];
+            const int64_t nseg = (T + kSeg - 1) / kSeg;
+            const int64_t rounds = (nseg + kProducers - 1) / kProducers;
+            // producer warp wib (1..7): the weights of segment sg into set `set`
+            auto produce = [&](int64_t sg, int set) {
+                double* buf = s_buf + ((int64_t)set * kProducers + (wib - 1)) * kSeg;
+                const int64_t t0 = sg * kSeg;
+                if (t0 >= T) return;  // uniform across the warp
+                int32_t z[kSegChunks], dz[kSegChunks];
+#pragma unroll
+                for (int c = 0; c < kSegChunks; ++c) {
+                    const int64_t e = t0 + 32 * c + lane;
+                    z[c] = e < T ? __ldg(a.lists + (E0 + e - a.e0)) : -1;
+                }
+#pragma unroll
+                for (int c = 0; c < kSegChunks; ++c) dz[c] = z[c] >= 0 ? __ldg(a.deg + z[c]) : 1;
+                // the slot of the lane's first term: the last p in [q0, q1) with lpos[p] <= E0 + e
+                const int64_t e_first = E0 + t0 + lane;
+                int64_t lo = q0, hi = q1 - 1;
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi + 1) >> 1;
+                    if (a.lpos[mid] <= e_first) lo = mid;
+                    else hi = mid - 1;
+                }
+                int64_t p = lo;
+                int64_t dxy = dx * (int64_t)a.deg[a.nb[p]];
+#pragma unroll
+                for (int c = 0; c < kSegChunks; ++c) {
+                    const int64_t e = t0 + 32 * c + lane;
+                    double w = 0.0;
+                    if (e < T) {
+                        bool moved = false;
+                        while (a.lpos[p + 1] <= E0 + e) {
+                            ++p;
+                            moved = true;
+                        }
+                        if (moved) dxy = dx * (int64_t)a.deg[a.nb[p]];
+                        w = 1.0 / (double)(dxy * (int64_t)dz[c]);
+                    }
+                    buf[32 * c + lane] = w;
+                }
+            };
+            double acc = 0.0;  // meaningful in warp 0
+            if (wib > 0) produce(wib - 1, 0);
+            __syncthreads();
+            for (int64_t r = 0; r < rounds; ++r) {
+                const int set = (int)(r & 1);
+                if (wib == 0) {
+                    for (int w = 0; w < kProducers; ++w) {
+                        const int64_t t0 = (r * kProducers + w) * kSeg;
+                        if (t0 >= T) break;
+                        const int cnt = T - t0 < kSeg ? (int)(T - t0) : kSeg;
+                        const double* bb = s_buf + ((int64_t)set * kProducers + w) * kSeg;
+#pragma unroll 8
+                        for (int k = 0; k < cnt; ++k) acc += bb[k];
+                    }
+                } else if (r + 1 < rounds) {
+                    produce((r + 1) * kProducers + wib - 1, set ^ 1);
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) a.pv[x] = acc;
+        }
+        __syncthreads();  // s_x is rewritten next
+    }
+}
+
 // Vertices of at least warp_min terms, keyed for a descending sort by term count.
 __global__ void k_big_keys(const int64_t* __restrict__ off, const int64_t* __restrict__ lpos, int64_t n,
-                           int64_t warp_min, uint64_t* __restrict__ keys, unsigned* __restrict__ nbig)
+                           int64_t warp_min, int64_t block_min, uint64_t* __restrict__ keys,
+                           unsigned* __restrict__ nbig)
 {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = lpos[off[v + 1]] - lpos[off[v]];
+        if (t >= block_min) atomicAdd(nbig + 1, 1u);
         if (t >= warp_min) {
             const uint64_t tc = t < 0xffffffffll ? (uint64_t)t : 0xffffffffull;
             keys[atomicAdd(nbig, 1u)] = ((0xffffffffull - tc) << 32) | (uint64_t)v;
@@ -396,23 +505,26 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
     int64_t* tmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(m2 + 1));
     uint64_t* keys = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
     uint64_t* alt = (uint64_t*)sc.get(sizeof(uint64_t) * (n + 1));
-    unsigned* d_nbig = (unsigned*)sc.get(sizeof(unsigned) * 2);
-    unsigned long long* next = (unsigned long long*)sc.get(sizeof(unsigned long long) * 2);
+    unsigned* d_nbig = (unsigned*)sc.get(sizeof(unsigned) * 2);  // [0] warp or block folds, [1] block folds
+    unsigned long long* next = (unsigned long long*)sc.get(sizeof(unsigned long long) * 2);  // [0] warps [1] blocks
     int64_t* d_x1 = (int64_t*)sc.get(sizeof(int64_t) * 2);
     if (!tmp || !keys || !alt || !d_nbig || !next || !d_x1) {
         set_error("device allocation failed (rows layout)");
         return RTR_ERR_CUDA;
     }
     exclusive_scan_i64(cgt, lpos, m2 + 1, nullptr, tmp, s);
+    // a warp from warp_min terms, a thread block from 64 x warp_min
     const int64_t warp_min = g->count_hub;
-    RTR_CUDA_TRY(cudaMemsetAsync(d_nbig, 0, sizeof(unsigned), s));
-    k_big_keys<<<grid_for(n, 256), 256, 0, s>>>(g->offsets, lpos, n, warp_min, keys, d_nbig);
+    const int64_t block_min = 64 * warp_min;
+    RTR_CUDA_TRY(cudaMemsetAsync(d_nbig, 0, 2 * sizeof(unsigned), s));
+    k_big_keys<<<grid_for(n, 256), 256, 0, s>>>(g->offsets, lpos, n, warp_min, block_min, keys, d_nbig);
     int64_t want = 0;
-    unsigned nbig = 0;
+    unsigned nb2[2] = {0, 0};
     RTR_CUDA_TRY(cudaMemcpyAsync(&want, lpos + m2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    RTR_CUDA_TRY(cudaMemcpyAsync(&nbig, d_nbig, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    RTR_CUDA_TRY(cudaMemcpyAsync(nb2, d_nbig, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     RTR_CUDA_TRY(cudaStreamSynchronize(s));
     g->launches += 2;
+    const unsigned nbig = nb2[0], nhuge = nb2[1];  // big[0, nhuge) take a block, the rest a warp
     int32_t* big = nullptr;
     if (nbig > 0) {
         void* rtmp = sc.get(radix_temp_bytes(nbig));
@@ -440,7 +552,12 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
     cudaEvent_t ready = nullptr, joined = nullptr;
     RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
     RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
-    float ms_fill = 0, ms_fold = 0, ms_warp = 0, ms_fill_l = 0, ms_fill_h = 0;
+    float ms_fill = 0, ms_fold = 0, ms_warp = 0, ms_fill_l = 0, ms_fill_h = 0, ms_block = 0;
+    // block folds: one per SM at most (kBlockFoldSmem of shared memory each)
+    int hub_grid = 148;
+    cudaDeviceGetAttribute(&hub_grid, cudaDevAttrMultiProcessorCount, g->device);
+    if (nhuge > 0) RTR_CUDA_TRY(cudaFuncSetAttribute(k_vfold_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)kBlockFoldSmem));
     int rc = RTR_OK;
     for (int64_t x0 = 0; x0 < n && rc == RTR_OK;) {
         int64_t x1 = n;
@@ -481,18 +598,25 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         ktime_end(g, KT_FILL_HEAVY);
         ktime_end(g, KT_TRI_FILL);
         FoldArgs fo{g->offsets, g->nbors, g->deg, lpos, e01[0], lists, g->pv, x0, x1, warp_min};
-        cudaMemsetAsync(next, 0, sizeof(unsigned long long), s);
+        cudaMemsetAsync(next, 0, 2 * sizeof(unsigned long long), s);
         ktime_begin(g, KT_VERTEX_FOLD);
+        // block folds on the second stream, concurrent with the warp and thread folds
         cudaEventRecord(ready, s);
         cudaStreamWaitEvent(g->side, ready, 0);
-        ktime_begin(g, KT_FOLD_WARP, g->side);
-        if (nbig > 0) k_vfold_warp<<<grid_for(1ll << 40, kFoldBlock, 8), kFoldBlock, 0, g->side>>>(fo, big, nbig, next);
-        ktime_end(g, KT_FOLD_WARP, g->side);
+        ktime_begin(g, KT_FOLD_BLOCK, g->side);
+        if (nhuge > 0)
+            k_vfold_block<<<(int)(nhuge < (unsigned)hub_grid ? nhuge : (unsigned)hub_grid), kFoldBlock,
+                            kBlockFoldSmem, g->side>>>(fo, big, nhuge, next + 1);
+        ktime_end(g, KT_FOLD_BLOCK, g->side);
         cudaEventRecord(joined, g->side);
+        ktime_begin(g, KT_FOLD_WARP);
+        if (nbig > nhuge)
+            k_vfold_warp<<<grid_for(1ll << 40, kFoldBlock, 8), kFoldBlock, 0, s>>>(fo, big + nhuge, nbig - nhuge, next);
+        ktime_end(g, KT_FOLD_WARP);
         k_vfold_thread<<<grid_for(x1 - x0, kFoldBlock), kFoldBlock, 0, s>>>(fo);
         cudaStreamWaitEvent(s, joined, 0);
         ktime_end(g, KT_VERTEX_FOLD);
-        g->launches += nbig > 0 ? 4 : 3;
+        g->launches += 1 + (nbig > nhuge ? 1 : 0) + (nhuge > 0 ? 1 : 0) + 2;
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {
             rc = cuda_fail(e, "rows-layout fill / fold launch", __FILE__, __LINE__);
@@ -505,6 +629,8 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         ktime_read(g, KT_TRI_FILL);
         ktime_read(g, KT_VERTEX_FOLD);
         ktime_read(g, KT_FOLD_WARP);
+        ktime_read(g, KT_FOLD_BLOCK);
+        ms_block += g->kms[KT_FOLD_BLOCK];
         ktime_read(g, KT_FILL_LIGHT);
         ktime_read(g, KT_FILL_HEAVY);
         ms_fill_l += g->kms[KT_FILL_LIGHT];
@@ -522,6 +648,7 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
     g->kms[KT_FOLD_WARP] = ms_warp;
     g->kms[KT_FILL_LIGHT] = ms_fill_l;
     g->kms[KT_FILL_HEAVY] = ms_fill_h;
+    g->kms[KT_FOLD_BLOCK] = ms_block;
     return rc;
 }
 

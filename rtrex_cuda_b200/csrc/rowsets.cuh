@@ -69,6 +69,69 @@ __device__ __forceinline__ void warp_scan(const int32_t* __restrict__ nb, int64_
     }
 }
 
+// Batched form of a warp_scan through table t of the longer row (whose
+// largest element is zmax): each step takes B chunks of 32 elements of S =
+// [s0, s1), with the next step's elements loaded ahead and the first bucket of
+// all 32*B lookups in flight at once; on_step(hit, x) then sees the step's B
+// chunks (lane k of chunk b holds element base + 32b + k), every lane, in
+// ascending order.  The walk stops at the first step whose first chunk lies
+// wholly above zmax.
+template <int B, typename F>
+__device__ __forceinline__ void warp_probe_walk(const RowSets& rs, int32_t t, const int32_t* __restrict__ nb,
+                                                int64_t s0, int64_t s1, int32_t zmax, int lane, F&& on_step)
+{
+    const int4* tb = reinterpret_cast<const int4*>(rs.slot + rs.toff[t]);
+    const int bits = rs.tbits[t];
+    const uint32_t mask = (1u << bits) - 1u;
+    int32_t xn[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        const int64_t p = s0 + 32 * b + lane;
+        xn[b] = p < s1 ? nb[p] : 0x7fffffff;
+    }
+    for (int64_t base = s0; base < s1; base += 32 * B) {
+        int32_t x[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            x[b] = xn[b];
+            const int64_t p = base + 32 * (B + b) + lane;
+            xn[b] = p < s1 ? nb[p] : 0x7fffffff;  // the next step, ahead of this one's lookups
+        }
+        if (__all_sync(0xffffffffu, x[0] > zmax)) break;
+        uint32_t bk[B];
+        int4 k0[B], k1[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            bk[b] = rs_hash(x[b], bits);
+            if (x[b] <= zmax) {
+                k0[b] = __ldg(tb + 2 * bk[b]);
+                k1[b] = __ldg(tb + 2 * bk[b] + 1);
+            } else {
+                k0[b] = k1[b] = make_int4(-1, -1, -1, -1);
+            }
+        }
+        bool hit[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int32_t z = x[b];
+            auto match = [&](const int4& p, const int4& q) {
+                return p.x == z || p.y == z || p.z == z || p.w == z || q.x == z || q.y == z || q.z == z || q.w == z;
+            };
+            bool h = z <= zmax && match(k0[b], k1[b]);
+            bool more = z <= zmax && !h && k1[b].w >= 0;  // the bucket is full: z may sit further on
+            uint32_t c = bk[b];
+            while (more) {
+                c = (c + 1u) & mask;
+                const int4 p = __ldg(tb + 2 * c), q = __ldg(tb + 2 * c + 1);
+                h = match(p, q);
+                more = !h && q.w >= 0;
+            }
+            hit[b] = h;
+        }
+        on_step(hit, x);
+    }
+}
+
 // Common neighbours z >= from of the rows of a and b, ascending: f(z).  One
 // thread.  The shorter row is walked and its elements looked up in the longer
 // row's hash set when that row has one; otherwise the rows merge or gallop

@@ -108,7 +108,8 @@ struct rtr_graph {
     // [0] k_edge_fold [1] k_tri_fill [2] k_vertex_fold [3] k_clean_units [4] k_extract_components
     // [5] decompose [6] k_edge_fold alone [7] k_edge_count_heavy alone [8] the rows
     // layout's warp perVertex fold (second stream, concurrent with the thread fold)
-    // [9] k_fill_light [10] k_fill_heavy (rows layout)
+    // [9] k_fill_light [10] k_fill_heavy [11] the block perVertex fold (rows layout; second
+    // stream, while [8] is then the warp fold alone on the graph's stream)
     static constexpr int kTimers = 12;
     cudaEvent_t kev[2 * kTimers] = {};
     float kms[kTimers] = {};
@@ -142,7 +143,8 @@ enum KernelTimer {
     KT_EDGE_HEAVY,
     KT_FOLD_WARP,
     KT_FILL_LIGHT,
-    KT_FILL_HEAVY
+    KT_FILL_HEAVY,
+    KT_FOLD_BLOCK
 };
 inline void ktime_begin(rtr_graph* g, int k, cudaStream_t s = nullptr)
 {
