@@ -137,6 +137,7 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
                        unsigned long long* __restrict__ total)
 {
     __shared__ double s_w[kHeavyEdgeBlock / 32][32];
+    __shared__ int32_t s_z[kHeavyEdgeBlock / 32][128];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t nh = *nheavy;
     const int64_t nwarps = (int64_t)gridDim.x * (kHeavyEdgeBlock / 32);
@@ -154,21 +155,32 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
         if (t >= 0) {
             // 4 chunks per step, their lookups and then their degrees in flight together
             constexpr int B = 4;
+            // perEdge: the step's hits, in order, are packed one per lane (ballot ranks), so that one
+            // pass of divisions serves all four chunks, and enter the chain by shuffle
+            const unsigned lt = (1u << lane) - 1u;
             warp_probe_walk<B>(rs, t, nb, u_short ? u0 : v0, u_short ? u1 : v1, nb[(u_short ? v1 : u1) - 1], lane,
                                [&](const bool (&hit)[B], const int32_t (&x)[B]) {
-                                   int32_t dz[B];
-#pragma unroll
-                                   for (int b = 0; b < B; ++b) dz[b] = (pe && hit[b]) ? deg[x[b]] : 1;
+                                   int tot = 0;
 #pragma unroll
                                    for (int b = 0; b < B; ++b) {
                                        c += hit[b] ? 1u : 0u;
                                        above += (hit[b] && x[b] > v) ? 1u : 0u;
                                        above_u += (hit[b] && x[b] > u) ? 1u : 0u;
-                                       if (pe) {
-                                           const double w = hit[b] ? 1.0 / (double)(duv * (int64_t)dz[b]) : 0.0;
-                                           fold_hits(hit[b], w, s_w[wib], lane, &acc, nullptr, 0);
-                                       }
+                                       const unsigned mb = __ballot_sync(0xffffffffu, hit[b]);
+                                       if (pe && hit[b]) s_z[wib][tot + __popc(mb & lt)] = x[b];
+                                       tot += __popc(mb);
                                    }
+                                   if (!pe || tot == 0) return;
+                                   __syncwarp();
+                                   for (int q0 = 0; q0 < tot; q0 += 32) {
+                                       const int j = q0 + lane;
+                                       const double w =
+                                           j < tot ? 1.0 / (double)(duv * (int64_t)deg[s_z[wib][j]]) : 0.0;
+                                       const int cc = tot - q0 < 32 ? tot - q0 : 32;
+#pragma unroll 4
+                                       for (int k = 0; k < cc; ++k) acc += __shfl_sync(0xffffffffu, w, k);
+                                   }
+                                   __syncwarp();
                                });
             if (pe && lane == 0) pe[i] = acc;
         } else if (pe) {

@@ -254,20 +254,22 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
 }
 
 // The largest vertices (at least block_min terms), a thread block each, from
-// the front of big[] (descending term count): warp 0 runs the add chain and
-// nothing else, warps 1..7 produce the weights.  The terms of x are cut into
-// segments of kSeg; round r gives the producers the next 7 segments, each lane
-// loading its 32 terms and their degrees with all loads in flight at once and
-// writing 32 weights to the segment's shared-memory buffer (set r&1), while
-// warp 0 adds the previous round's 7 segments in order.  One block barrier per
-// round; the chain costs one double add per term.
-constexpr int kSeg = 1024;
+// the front of big[] (descending term count), two blocks per SM: warp 0 runs
+// the add chain and nothing else, warps 1..7 produce the weights.  The terms of
+// x are cut into segments of kSeg; round r gives the producers the next 7
+// segments, each lane loading its 16 terms and their degrees with all loads in
+// flight at once and writing 16 weights to the segment's shared-memory buffer
+// (set r&1), while warp 0 adds the previous round's 7 segments in order,
+// taking them 32 at a time into registers and by shuffle into the chain.  One
+// block barrier per round; the chain costs about one double add latency per
+// term.
+constexpr int kSeg = 512;
 constexpr int kSegChunks = kSeg / 32;
 constexpr int kProducers = kFoldBlock / 32 - 1;
 constexpr size_t kBlockFoldSmem = sizeof(double) * 2 * kProducers * kSeg;
 
-__global__ void __launch_bounds__(kFoldBlock) k_vfold_block(FoldArgs a, const int32_t* __restrict__ huge,
-                                                             int64_t nhuge, unsigned long long* __restrict__ next)
+__global__ void __launch_bounds__(kFoldBlock, 2) k_vfold_block(FoldArgs a, const int32_t* __restrict__ huge,
+                                                                int64_t nhuge, unsigned long long* __restrict__ next)
 {
     extern __shared__ double s_buf[];  // [2][kProducers][kSeg]
     __shared__ int64_t s_x;
@@ -286,6 +288,7 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_block(FoldArgs a, const in
             const int64_t dx = a.deg[x];
             const int64_t nseg = (T + kSeg - 1) / kSeg;
             const int64_t rounds = (nseg + kProducers - 1) / kProducers;
+            int64_t hint = q0;  // a producer's segments ascend: the slot its last one began in
             // producer warp wib (1..7): the weights of segment sg into set `set`
             auto produce = [&](int64_t sg, int set) {
                 double* buf = s_buf + ((int64_t)set * kProducers + (wib - 1)) * kSeg;
@@ -299,14 +302,25 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_block(FoldArgs a, const in
                 }
 #pragma unroll
                 for (int c = 0; c < kSegChunks; ++c) dz[c] = z[c] >= 0 ? __ldg(a.deg + z[c]) : 1;
-                // the slot of the lane's first term: the last p in [q0, q1) with lpos[p] <= E0 + e
-                const int64_t e_first = E0 + t0 + lane;
-                int64_t lo = q0, hi = q1 - 1;
-                while (lo < hi) {
+                // the slot of term t0 (the last p with lpos[p] <= E0 + t0): gallop from the hint, then bisect
+                const int64_t target = E0 + t0;
+                int64_t lo = hint, hi = q1 - 1;  // lpos[lo] <= target < lpos[q1]
+                for (int64_t step = 1;; step <<= 1) {
+                    const int64_t probe = lo + step;
+                    if (probe > hi) break;
+                    if (a.lpos[probe] <= target) {
+                        lo = probe;
+                    } else {
+                        hi = probe - 1;
+                        break;
+                    }
+                }
+                while (lo < hi) {  // the answer is in [lo, hi]
                     const int64_t mid = (lo + hi + 1) >> 1;
-                    if (a.lpos[mid] <= e_first) lo = mid;
+                    if (a.lpos[mid] <= target) lo = mid;
                     else hi = mid - 1;
                 }
+                hint = lo;
                 int64_t p = lo;
                 int64_t dxy = dx * (int64_t)a.deg[a.nb[p]];
 #pragma unroll
@@ -331,13 +345,23 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_block(FoldArgs a, const in
             for (int64_t r = 0; r < rounds; ++r) {
                 const int set = (int)(r & 1);
                 if (wib == 0) {
+                    // lane k holds term k of the next 32; the chain takes them by shuffle
                     for (int w = 0; w < kProducers; ++w) {
                         const int64_t t0 = (r * kProducers + w) * kSeg;
                         if (t0 >= T) break;
                         const int cnt = T - t0 < kSeg ? (int)(T - t0) : kSeg;
                         const double* bb = s_buf + ((int64_t)set * kProducers + w) * kSeg;
-#pragma unroll 8
-                        for (int k = 0; k < cnt; ++k) acc += bb[k];
+                        double v = lane < cnt ? bb[lane] : 0.0;
+                        for (int k0 = 0; k0 < cnt; k0 += 32) {
+                            const double vn = k0 + 32 + lane < cnt ? bb[k0 + 32 + lane] : 0.0;
+                            const int c = cnt - k0 < 32 ? cnt - k0 : 32;
+#pragma unroll
+                            for (int t = 0; t < 32; ++t) {
+                                const double y = __shfl_sync(0xffffffffu, v, t);
+                                if (t < c) acc += y;
+                            }
+                            v = vn;
+                        }
                     }
                 } else if (r + 1 < rounds) {
                     produce((r + 1) * kProducers + wib - 1, set ^ 1);
@@ -553,9 +577,10 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
     RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
     RTR_CUDA_TRY(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
     float ms_fill = 0, ms_fold = 0, ms_warp = 0, ms_fill_l = 0, ms_fill_h = 0, ms_block = 0;
-    // block folds: one per SM at most (kBlockFoldSmem of shared memory each)
+    // block folds: two per SM (kBlockFoldSmem of shared memory each)
     int hub_grid = 148;
     cudaDeviceGetAttribute(&hub_grid, cudaDevAttrMultiProcessorCount, g->device);
+    hub_grid *= 2;
     if (nhuge > 0) RTR_CUDA_TRY(cudaFuncSetAttribute(k_vfold_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                      (int)kBlockFoldSmem));
     int rc = RTR_OK;
