@@ -256,87 +256,73 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
 // The largest vertices (at least block_min terms), a thread block each, from
 // the front of big[] (descending term count), two blocks per SM: warp 0 runs
 // the add chain and nothing else, warps 1..7 produce the weights.  The terms of
-// x are cut into segments of kSeg; round r gives the producers the next 7
-// segments, each lane loading its 16 terms and their degrees with all loads in
-// flight at once and writing 16 weights to the segment's shared-memory buffer
-// (set r&1), while warp 0 adds the previous round's 7 segments in order,
-// taking them 32 at a time into registers and by shuffle into the chain.  One
-// block barrier per round; the chain costs about one double add latency per
-// term.
-constexpr int kSeg = 512;
-constexpr int kSegChunks = kSeg / 32;
+// x are cut into segments of kSeg, whose first slots k_seg_slots finds ahead of
+// time; round r gives the producers the next 7 segments, each lane loading 12
+// terms and their degrees at a time with all loads in flight at once and
+// writing the weights to the segment's shared-memory buffer (set r&1), while
+// warp 0 adds the previous round's 7 segments in order, taking them 32 at a
+// time into registers and by shuffle into the chain.  One block barrier per
+// round; the chain costs about one double add latency per term.
+constexpr int kSeg = 768;
+constexpr int kHalfChunks = kSeg / 64;  // a producer takes its segment in two halves of 12 chunks
 constexpr int kProducers = kFoldBlock / 32 - 1;
 constexpr size_t kBlockFoldSmem = sizeof(double) * 2 * kProducers * kSeg;
 
-__global__ void __launch_bounds__(kFoldBlock, 2) k_vfold_block(FoldArgs a, const int32_t* __restrict__ huge,
-                                                                int64_t nhuge, unsigned long long* __restrict__ next)
+__global__ void __launch_bounds__(kFoldBlock, 2)
+    k_vfold_block(FoldArgs a, const int32_t* __restrict__ huge, int64_t nhuge, const int64_t* __restrict__ segoff,
+                  const int32_t* __restrict__ segslot, unsigned long long* __restrict__ next)
 {
     extern __shared__ double s_buf[];  // [2][kProducers][kSeg]
-    __shared__ int64_t s_x;
+    __shared__ int64_t s_h;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     while (true) {
         if (threadIdx.x == 0) {
             const unsigned long long b = atomicAdd(next, 1ull);
-            s_x = (int64_t)b < nhuge ? huge[b] : -1;
+            s_h = (int64_t)b < nhuge ? (int64_t)b : -1;
         }
         __syncthreads();
-        const int64_t x = s_x;
-        if (x < 0) break;  // uniform across the block
+        const int64_t h = s_h;
+        if (h < 0) break;  // uniform across the block
+        const int64_t x = huge[h];
         if (x >= a.x0 && x < a.x1) {
             const int64_t q0 = a.off[x], q1 = a.off[x + 1];
             const int64_t E0 = a.lpos[q0], T = a.lpos[q1] - E0;
             const int64_t dx = a.deg[x];
             const int64_t nseg = (T + kSeg - 1) / kSeg;
             const int64_t rounds = (nseg + kProducers - 1) / kProducers;
-            int64_t hint = q0;  // a producer's segments ascend: the slot its last one began in
+            const int32_t* sslot = segslot + segoff[h];
             // producer warp wib (1..7): the weights of segment sg into set `set`
             auto produce = [&](int64_t sg, int set) {
                 double* buf = s_buf + ((int64_t)set * kProducers + (wib - 1)) * kSeg;
                 const int64_t t0 = sg * kSeg;
                 if (t0 >= T) return;  // uniform across the warp
-                int32_t z[kSegChunks], dz[kSegChunks];
+                int64_t p = q0 + sslot[sg];  // the slot of term t0
+                int64_t dxy = -1;
+#pragma unroll 1
+                for (int half = 0; half < 2; ++half) {
+                    const int64_t h0 = t0 + half * (kSeg / 2);
+                    int32_t z[kHalfChunks], dz[kHalfChunks];
 #pragma unroll
-                for (int c = 0; c < kSegChunks; ++c) {
-                    const int64_t e = t0 + 32 * c + lane;
-                    z[c] = e < T ? __ldg(a.lists + (E0 + e - a.e0)) : -1;
-                }
-#pragma unroll
-                for (int c = 0; c < kSegChunks; ++c) dz[c] = z[c] >= 0 ? __ldg(a.deg + z[c]) : 1;
-                // the slot of term t0 (the last p with lpos[p] <= E0 + t0): gallop from the hint, then bisect
-                const int64_t target = E0 + t0;
-                int64_t lo = hint, hi = q1 - 1;  // lpos[lo] <= target < lpos[q1]
-                for (int64_t step = 1;; step <<= 1) {
-                    const int64_t probe = lo + step;
-                    if (probe > hi) break;
-                    if (a.lpos[probe] <= target) {
-                        lo = probe;
-                    } else {
-                        hi = probe - 1;
-                        break;
+                    for (int c = 0; c < kHalfChunks; ++c) {
+                        const int64_t e = h0 + 32 * c + lane;
+                        z[c] = e < T ? __ldg(a.lists + (E0 + e - a.e0)) : -1;
                     }
-                }
-                while (lo < hi) {  // the answer is in [lo, hi]
-                    const int64_t mid = (lo + hi + 1) >> 1;
-                    if (a.lpos[mid] <= target) lo = mid;
-                    else hi = mid - 1;
-                }
-                hint = lo;
-                int64_t p = lo;
-                int64_t dxy = dx * (int64_t)a.deg[a.nb[p]];
 #pragma unroll
-                for (int c = 0; c < kSegChunks; ++c) {
-                    const int64_t e = t0 + 32 * c + lane;
-                    double w = 0.0;
-                    if (e < T) {
-                        bool moved = false;
-                        while (a.lpos[p + 1] <= E0 + e) {
-                            ++p;
-                            moved = true;
+                    for (int c = 0; c < kHalfChunks; ++c) dz[c] = z[c] >= 0 ? __ldg(a.deg + z[c]) : 1;
+#pragma unroll
+                    for (int c = 0; c < kHalfChunks; ++c) {
+                        const int64_t e = h0 + 32 * c + lane;
+                        double w = 0.0;
+                        if (e < T) {
+                            while (a.lpos[p + 1] <= E0 + e) {
+                                ++p;
+                                dxy = -1;
+                            }
+                            if (dxy < 0) dxy = dx * (int64_t)a.deg[a.nb[p]];
+                            w = 1.0 / (double)(dxy * (int64_t)dz[c]);
                         }
-                        if (moved) dxy = dx * (int64_t)a.deg[a.nb[p]];
-                        w = 1.0 / (double)(dxy * (int64_t)dz[c]);
+                        buf[half * (kSeg / 2) + 32 * c + lane] = w;
                     }
-                    buf[32 * c + lane] = w;
                 }
             };
             double acc = 0.0;  // meaningful in warp 0
@@ -370,7 +356,44 @@ __global__ void __launch_bounds__(kFoldBlock, 2) k_vfold_block(FoldArgs a, const
             }
             if (threadIdx.x == 0) a.pv[x] = acc;
         }
-        __syncthreads();  // s_x is rewritten next
+        __syncthreads();  // s_h is rewritten next
+    }
+}
+
+// Segments of the block-folded vertices: how many each has, and the slot (from
+// the row's start) that holds each segment's first term.
+__global__ void k_seg_counts(const int64_t* __restrict__ off, const int64_t* __restrict__ lpos,
+                             const int32_t* __restrict__ huge, int64_t nhuge, int64_t* __restrict__ cnt)
+{
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h <= nhuge; h += (int64_t)gridDim.x * blockDim.x) {
+        if (h == nhuge) {
+            cnt[h] = 0;
+            continue;
+        }
+        const int64_t x = huge[h];
+        const int64_t T = lpos[off[x + 1]] - lpos[off[x]];
+        cnt[h] = (T + kSeg - 1) / kSeg;
+    }
+}
+
+__global__ void k_seg_slots(const int64_t* __restrict__ off, const int64_t* __restrict__ lpos,
+                            const int32_t* __restrict__ huge, int64_t nhuge, const int64_t* __restrict__ segoff,
+                            int32_t* __restrict__ segslot)
+{
+    for (int64_t h = blockIdx.x; h < nhuge; h += gridDim.x) {
+        const int64_t x = huge[h];
+        const int64_t q0 = off[x], q1 = off[x + 1], E0 = lpos[q0];
+        const int64_t ns = segoff[h + 1] - segoff[h];
+        for (int64_t sg = threadIdx.x; sg < ns; sg += blockDim.x) {
+            const int64_t target = E0 + sg * kSeg;
+            int64_t lo = q0, hi = q1 - 1;  // the last p with lpos[p] <= target
+            while (lo < hi) {
+                const int64_t mid = (lo + hi + 1) >> 1;
+                if (lpos[mid] <= target) lo = mid;
+                else hi = mid - 1;
+            }
+            segslot[segoff[h] + sg] = (int32_t)(lo - q0);
+        }
     }
 }
 
@@ -561,6 +584,30 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         k_low_ids<<<grid_for(nbig, 256), 256, 0, s>>>(sorted, nbig, big);
         g->launches += 1 + 3 * 8;
     }
+    // the block-folded vertices' segments and the slot each one starts in
+    int64_t* segoff = nullptr;
+    int32_t* segslot = nullptr;
+    if (nhuge > 0) {
+        int64_t* scnt = (int64_t*)sc.get(sizeof(int64_t) * (nhuge + 1));
+        segoff = (int64_t*)sc.get(sizeof(int64_t) * (nhuge + 1));
+        int64_t* stmp = (int64_t*)sc.get(sizeof(int64_t) * scan_temp_elems(nhuge + 1));
+        if (!scnt || !segoff || !stmp) {
+            set_error("device allocation failed (rows layout)");
+            return RTR_ERR_CUDA;
+        }
+        k_seg_counts<<<grid_for(nhuge + 1, 256), 256, 0, s>>>(g->offsets, lpos, big, nhuge, scnt);
+        exclusive_scan_i64(scnt, segoff, nhuge + 1, nullptr, stmp, s);
+        int64_t nseg = 0;
+        RTR_CUDA_TRY(cudaMemcpyAsync(&nseg, segoff + nhuge, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        RTR_CUDA_TRY(cudaStreamSynchronize(s));
+        segslot = (int32_t*)sc.get(sizeof(int32_t) * (nseg + 1));
+        if (!segslot) {
+            set_error("device allocation failed (rows layout)");
+            return RTR_ERR_CUDA;
+        }
+        k_seg_slots<<<grid_for(1ll << 40, 256, 4), 256, 0, s>>>(g->offsets, lpos, big, nhuge, segoff, segslot);
+        g->launches += 3;
+    }
     // the lists: all of them when they fit in the free HBM (less 1 GiB), else windows of whole rows
     size_t free_b = 0, total_b = 0;
     RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
@@ -631,7 +678,7 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         ktime_begin(g, KT_FOLD_BLOCK, g->side);
         if (nhuge > 0)
             k_vfold_block<<<(int)(nhuge < (unsigned)hub_grid ? nhuge : (unsigned)hub_grid), kFoldBlock,
-                            kBlockFoldSmem, g->side>>>(fo, big, nhuge, next + 1);
+                            kBlockFoldSmem, g->side>>>(fo, big, nhuge, segoff, segslot, next + 1);
         ktime_end(g, KT_FOLD_BLOCK, g->side);
         cudaEventRecord(joined, g->side);
         ktime_begin(g, KT_FOLD_WARP);
