@@ -14,12 +14,13 @@
 // slot (x,y), cgt = #{z in N(x) & N(y) : z > y} -- the number of terms slot
 // (x,y) adds to perVertex[x].  This file makes perVertex from that:
 //   lists     the exclusive scan of cgt gives every slot a list of its z > y,
-//             4 bytes each (3 per triangle: ~124 GB at R-MAT scale 24).
+//             4 bytes each (3 per triangle: ~124 GB at R-MAT scale 24); an
+//             entry holds deg z, all that the fold needs of z.
 //             Slots are taken in windows of whole rows that fit in the free
 //             HBM (one window when everything fits).
 //   fill      one more intersection per edge (u < v) restricted to z > u
-//             writes both slots' lists in ascending z: z > u to slot (v,u),
-//             z > v to slot (u,v).  k_fill_light: a thread per light edge;
+//             writes both slots' lists in ascending z: deg z for z > u to slot
+//             (v,u), for z > v to slot (u,v).  k_fill_light: a thread per light edge;
 //             k_fill_heavy: a warp per heavy edge, hits ranked by ballot.
 //   fold      perVertex[x] = the left fold of x's slots' lists in slot order
 //             (y ascending), each in z order -- exactly commonNbr's order.
@@ -78,8 +79,9 @@ __global__ void __launch_bounds__(kFillBlock) k_fill_light(FillArgs a)
         int64_t qi = a.lpos[i] - a.e0, qr = a.lpos[r] - a.e0;
         const int64_t qi1 = a.lpos[i + 1] - a.e0, qr1 = a.lpos[r + 1] - a.e0;
         thread_common(a.rs, a.off, a.nb, u, v, wr ? u + 1 : v + 1, a.gallop, [&](int32_t z) {
-            if (wr && qr < qr1) a.lists[qr++] = z;
-            if (wi && z > v && qi < qi1) a.lists[qi++] = z;
+            const int32_t dz = a.deg[z];
+            if (wr && qr < qr1) a.lists[qr++] = dz;
+            if (wi && z > v && qi < qi1) a.lists[qi++] = dz;
         });
     }
 }
@@ -105,26 +107,30 @@ __global__ void __launch_bounds__(kHeavyBlock) k_fill_heavy(FillArgs a, const in
         const bool u_short = u1 - u0 <= v1 - v0;
         const int64_t s1 = u_short ? u1 : v1;
         const int64_t s0 = lower_bound_row(a.nb, u_short ? u0 : v0, s1, from);
-        auto emit = [&](bool hit, int32_t z) {
+        auto emit = [&](bool hit, int32_t z, int32_t dz) {
             const bool to_r = hit && wr, to_i = hit && wi && z > v;
             const unsigned mr = __ballot_sync(0xffffffffu, to_r);
             const unsigned mi = __ballot_sync(0xffffffffu, to_i);
             const int64_t wr_at = qr + __popc(mr & lt), wi_at = qi + __popc(mi & lt);
-            if (to_r && wr_at < qr1) a.lists[wr_at] = z;
-            if (to_i && wi_at < qi1) a.lists[wi_at] = z;
+            if (to_r && wr_at < qr1) a.lists[wr_at] = dz;
+            if (to_i && wi_at < qi1) a.lists[wi_at] = dz;
             qr += __popc(mr);
             qi += __popc(mi);
         };
         const int32_t t = rs_table(a.rs, u_short ? v : u);
         if (t >= 0) {
-            constexpr int B = 4;  // 4 chunks per step, their lookups in flight together
+            constexpr int B = 4;  // 4 chunks per step, their lookups (then degrees) in flight together
             warp_probe_walk<B>(a.rs, t, a.nb, s0, s1, a.nb[(u_short ? v1 : u1) - 1], lane,
                                [&](const bool (&hit)[B], const int32_t (&x)[B]) {
+                                   int32_t dz[B];
 #pragma unroll
-                                   for (int b = 0; b < B; ++b) emit(hit[b], x[b]);
+                                   for (int b = 0; b < B; ++b) dz[b] = hit[b] ? a.deg[x[b]] : 0;
+#pragma unroll
+                                   for (int b = 0; b < B; ++b) emit(hit[b], x[b], dz[b]);
                                });
         } else {
-            warp_walk(a.rs, a.off, a.nb, s0, s1, u_short ? v : u, u_short ? v0 : u0, u_short ? v1 : u1, lane, emit);
+            warp_walk(a.rs, a.off, a.nb, s0, s1, u_short ? v : u, u_short ? v0 : u0, u_short ? v1 : u1, lane,
+                      [&](bool hit, int32_t z) { emit(hit, z, hit ? a.deg[z] : 0); });
         }
     }
 }
@@ -159,7 +165,7 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_thread(FoldArgs a)
             const int64_t e1 = a.lpos[p + 1];
             if (e1 == e) continue;
             const int64_t dxy = dx * (int64_t)a.deg[a.nb[p]];
-            for (; e < e1; ++e) acc += 1.0 / (double)(dxy * (int64_t)a.deg[a.lists[e - a.e0]]);
+            for (; e < e1; ++e) acc += 1.0 / (double)(dxy * (int64_t)a.lists[e - a.e0]);
         }
         a.pv[x] = acc;
     }
@@ -199,26 +205,18 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
             const int64_t dxy = (valid && len > 0) ? dx * (int64_t)a.deg[a.nb[p]] : 0;
             const int64_t base = a.lpos[g0] - a.e0;
             // Software pipeline over blocks of 4 chunks (128 terms): the lanes' terms
-            // are loaded two blocks ahead and their degrees one block ahead of the
-            // add chain, so the chain does not wait on either load.
-            auto zload = [&](int64_t k0) -> int32_t {
+            // (the degrees of their z) are loaded one block ahead of the add chain.
+            auto dload = [&](int64_t k0) -> int32_t {
                 const int64_t e = k0 + lane;
-                return e < G ? __ldg(a.lists + base + e) : -1;
+                return e < G ? __ldg(a.lists + base + e) : 1;
             };
-            auto dload = [&](int32_t z) -> int32_t { return z >= 0 ? __ldg(a.deg + z) : 1; };
-            int32_t zA[4], zB[4], dA[4];
+            int32_t dA[4];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) zA[c] = zload(32 * c);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) zB[c] = zload(128 + 32 * c);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) dA[c] = dload(zA[c]);
+            for (int c = 0; c < 4; ++c) dA[c] = dload(32 * c);
             for (int64_t b0 = 0; b0 < G; b0 += 128) {
-                int32_t zC[4], dB[4];
+                int32_t dB[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) zC[c] = zload(b0 + 256 + 32 * c);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) dB[c] = dload(zB[c]);
+                for (int c = 0; c < 4; ++c) dB[c] = dload(b0 + 128 + 32 * c);
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
                     const int64_t k0 = b0 + 32 * c;
@@ -242,11 +240,7 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
                     }
                 }
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    zA[c] = zB[c];
-                    zB[c] = zC[c];
-                    dA[c] = dB[c];
-                }
+                for (int c = 0; c < 4; ++c) dA[c] = dB[c];
             }
         }
         if (lane == 0) a.pv[x] = acc;
@@ -291,35 +285,53 @@ __global__ void __launch_bounds__(kFoldBlock, 2)
             const int64_t nseg = (T + kSeg - 1) / kSeg;
             const int64_t rounds = (nseg + kProducers - 1) / kProducers;
             const int32_t* sslot = segslot + segoff[h];
-            // producer warp wib (1..7): the weights of segment sg into set `set`
+            // producer warp wib (1..7): the weights of segment sg into set `set`.  Lane j
+            // holds the term end and dx*dy of slot gp+j; a term's slot is the number of
+            // lanes whose end is <= it (a five-step shuffle search).
             auto produce = [&](int64_t sg, int set) {
                 double* buf = s_buf + ((int64_t)set * kProducers + (wib - 1)) * kSeg;
                 const int64_t t0 = sg * kSeg;
                 if (t0 >= T) return;  // uniform across the warp
-                int64_t p = q0 + sslot[sg];  // the slot of term t0
-                int64_t dxy = -1;
+                const int64_t t1 = t0 + kSeg < T ? t0 + kSeg : T;
+                int64_t gp = q0 + sslot[sg];  // the slot of term t0
+                int64_t endj = 0, dyj = 0, gend = 0;
+                auto load_group = [&]() {
+                    const int64_t sl = gp + lane;
+                    endj = sl < q1 ? a.lpos[sl + 1] - E0 : 0x7fffffffffffffffll;
+                    dyj = sl < q1 ? dx * (int64_t)a.deg[a.nb[sl]] : 0;
+                    gend = __shfl_sync(0xffffffffu, endj, 31);  // the group holds the terms below gend
+                };
+                load_group();
 #pragma unroll 1
                 for (int half = 0; half < 2; ++half) {
                     const int64_t h0 = t0 + half * (kSeg / 2);
-                    int32_t z[kHalfChunks], dz[kHalfChunks];
+                    int32_t dz[kHalfChunks];
 #pragma unroll
                     for (int c = 0; c < kHalfChunks; ++c) {
                         const int64_t e = h0 + 32 * c + lane;
-                        z[c] = e < T ? __ldg(a.lists + (E0 + e - a.e0)) : -1;
+                        dz[c] = e < t1 ? __ldg(a.lists + (E0 + e - a.e0)) : 1;
                     }
-#pragma unroll
-                    for (int c = 0; c < kHalfChunks; ++c) dz[c] = z[c] >= 0 ? __ldg(a.deg + z[c]) : 1;
 #pragma unroll
                     for (int c = 0; c < kHalfChunks; ++c) {
                         const int64_t e = h0 + 32 * c + lane;
                         double w = 0.0;
-                        if (e < T) {
-                            while (a.lpos[p + 1] <= E0 + e) {
-                                ++p;
-                                dxy = -1;
+                        bool need = e < t1;
+                        while (__any_sync(0xffffffffu, need)) {  // ends: the last slot's end is T
+                            int q = 0;
+#pragma unroll
+                            for (int step = 16; step > 0; step >>= 1) {
+                                const int64_t cq = __shfl_sync(0xffffffffu, endj, q + step - 1);
+                                if (cq <= e) q += step;
                             }
-                            if (dxy < 0) dxy = dx * (int64_t)a.deg[a.nb[p]];
-                            w = 1.0 / (double)(dxy * (int64_t)dz[c]);
+                            const int64_t dq = __shfl_sync(0xffffffffu, dyj, q & 31);
+                            if (need && e < gend) {
+                                w = 1.0 / (double)(dq * (int64_t)dz[c]);
+                                need = false;
+                            }
+                            if (__any_sync(0xffffffffu, need)) {
+                                gp += 32;
+                                load_group();
+                            }
                         }
                         buf[half * (kSeg / 2) + 32 * c + lane] = w;
                     }
