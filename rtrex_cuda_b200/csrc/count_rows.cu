@@ -248,15 +248,15 @@ __global__ void __launch_bounds__(kFoldBlock) k_vfold_warp(FoldArgs a, const int
 }
 
 // The largest vertices (at least block_min terms), a thread block each, from
-// the front of big[] (descending term count), two blocks per SM: warp 0 runs
-// the add chain and nothing else, warps 1..7 produce the weights.  The terms of
+// the front of big[] (descending term count), two blocks per SM: one warp runs
+// the add chain and nothing else, the other seven produce the weights.  The terms of
 // x are cut into segments of kSeg, whose first slots k_seg_slots finds ahead of
 // time; round r gives the producers the next 7 segments, each lane loading 12
 // terms and their degrees at a time with all loads in flight at once and
 // writing the weights to the segment's shared-memory buffer (set r&1), while
-// warp 0 adds the previous round's 7 segments in order, taking them 32 at a
-// time into registers and by shuffle into the chain.  One block barrier per
-// round; the chain costs about one double add latency per term.
+// the chain warp adds the previous round's 7 segments in order, from 16-byte
+// shared-memory loads issued ahead of the adds.  One block barrier per round;
+// the chain costs about one double add latency per term.
 constexpr int kSeg = 768;
 constexpr int kHalfChunks = kSeg / 64;  // a producer takes its segment in two halves of 12 chunks
 constexpr int kProducers = kFoldBlock / 32 - 1;
@@ -269,6 +269,10 @@ __global__ void __launch_bounds__(kFoldBlock, 2)
     extern __shared__ double s_buf[];  // [2][kProducers][kSeg]
     __shared__ int64_t s_h;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    // the chain warp: picked by block index, so that the chains of the blocks an SM holds tend to
+    // sit on different schedulers; the other warps are producers 0..6 (pid < 0: the chain warp)
+    const int chain = (int)(blockIdx.x & 3);
+    const int pid = wib == chain ? -1 : (wib < chain ? wib : wib - 1);
     while (true) {
         if (threadIdx.x == 0) {
             const unsigned long long b = atomicAdd(next, 1ull);
@@ -285,11 +289,11 @@ __global__ void __launch_bounds__(kFoldBlock, 2)
             const int64_t nseg = (T + kSeg - 1) / kSeg;
             const int64_t rounds = (nseg + kProducers - 1) / kProducers;
             const int32_t* sslot = segslot + segoff[h];
-            // producer warp wib (1..7): the weights of segment sg into set `set`.  Lane j
+            // producer pid (0..6): the weights of segment sg into set `set`.  Lane j
             // holds the term end and dx*dy of slot gp+j; a term's slot is the number of
             // lanes whose end is <= it (a five-step shuffle search).
             auto produce = [&](int64_t sg, int set) {
-                double* buf = s_buf + ((int64_t)set * kProducers + (wib - 1)) * kSeg;
+                double* buf = s_buf + ((int64_t)set * kProducers + pid) * kSeg;
                 const int64_t t0 = sg * kSeg;
                 if (t0 >= T) return;  // uniform across the warp
                 const int64_t t1 = t0 + kSeg < T ? t0 + kSeg : T;
@@ -337,35 +341,41 @@ __global__ void __launch_bounds__(kFoldBlock, 2)
                     }
                 }
             };
-            double acc = 0.0;  // meaningful in warp 0
-            if (wib > 0) produce(wib - 1, 0);
+            double acc = 0.0;  // meaningful in the chain warp
+            if (pid >= 0) produce(pid, 0);
             __syncthreads();
             for (int64_t r = 0; r < rounds; ++r) {
                 const int set = (int)(r & 1);
-                if (wib == 0) {
-                    // lane k holds term k of the next 32; the chain takes them by shuffle
+                if (pid < 0) {
+                    // 16-byte broadcast loads, issued ahead of the adds (no shuffles: a double
+                    // shuffle is two instructions)
                     for (int w = 0; w < kProducers; ++w) {
                         const int64_t t0 = (r * kProducers + w) * kSeg;
                         if (t0 >= T) break;
                         const int cnt = T - t0 < kSeg ? (int)(T - t0) : kSeg;
                         const double* bb = s_buf + ((int64_t)set * kProducers + w) * kSeg;
-                        double v = lane < cnt ? bb[lane] : 0.0;
-                        for (int k0 = 0; k0 < cnt; k0 += 32) {
-                            const double vn = k0 + 32 + lane < cnt ? bb[k0 + 32 + lane] : 0.0;
-                            const int c = cnt - k0 < 32 ? cnt - k0 : 32;
-#pragma unroll
-                            for (int t = 0; t < 32; ++t) {
-                                const double y = __shfl_sync(0xffffffffu, v, t);
-                                if (t < c) acc += y;
-                            }
-                            v = vn;
+                        const double2* b2 = reinterpret_cast<const double2*>(bb);
+                        int k = 0;
+#pragma unroll 4
+                        for (; k + 8 <= cnt; k += 8) {
+                            const double2 p0 = b2[k / 2], p1 = b2[k / 2 + 1], p2 = b2[k / 2 + 2], p3 = b2[k / 2 + 3];
+                            acc += p0.x;
+                            acc += p0.y;
+                            acc += p1.x;
+                            acc += p1.y;
+                            acc += p2.x;
+                            acc += p2.y;
+                            acc += p3.x;
+                            acc += p3.y;
                         }
+                        for (; k < cnt; ++k) acc += bb[k];
                     }
                 } else if (r + 1 < rounds) {
-                    produce((r + 1) * kProducers + wib - 1, set ^ 1);
+                    produce((r + 1) * kProducers + pid, set ^ 1);
                 }
                 __syncthreads();
             }
+            if (pid < 0 && lane == 0) a.pv[x] = acc;
             if (threadIdx.x == 0) a.pv[x] = acc;
         }
         __syncthreads();  // s_h is rewritten next
