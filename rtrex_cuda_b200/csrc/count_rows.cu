@@ -376,7 +376,6 @@ __global__ void __launch_bounds__(kFoldBlock, 2)
                 __syncthreads();
             }
             if (pid < 0 && lane == 0) a.pv[x] = acc;
-            if (threadIdx.x == 0) a.pv[x] = acc;
         }
         __syncthreads();  // s_h is rewritten next
     }
