@@ -76,7 +76,6 @@ struct RoundSmem {
     unsigned hkey[kHashSlots];       // claimed cell (forward rank)
     unsigned hown[kHashSlots];       // smallest claiming window position
     double hacc[kHashSlots];         // sum of the claiming triangles' weights
-    double sw[kRoundWarps][32];      // per-warp live weights, packed in triangle order
     RoundCtl ctl[2];
     int wcnt[kRoundWarps];           // per-warp counts of a refill's kept seeds
     int np_solo;                     // pend count after a solo pop
@@ -207,7 +206,7 @@ __device__ void solo_pop(const RoundArgs& a, RoundSmem& S, const StackEntry& c, 
     const PairSide ps = pair_side(c);
     const EdgeRec* r = a.rec + c.e;
     const unsigned long long ow = *reinterpret_cast<const unsigned long long*>(&r->cnt);
-    double acc_e = r->pe;
+    const double pe_e = r->pe;
     const uint32_t s_e = (uint32_t)(ow >> 32) & SS_SUP;
     int nl_total = 0;
     if (s_e > 0) {
@@ -242,13 +241,10 @@ __device__ void solo_pop(const RoundArgs& a, RoundSmem& S, const StackEntry& c, 
             const unsigned b1 = __ballot_sync(kFull, f1), b2 = __ballot_sync(kFull, f2);
             if (live) {
                 const int k = __popc(lm & lt);
-                S.sw[0][k] = t.wgt;
                 a.wbuf[c.t0 + nl_total + k] = t.wgt;
                 a.zbuf[c.t0 + nl_total + k] = t.z;
             }
-            __syncwarp();
             const int nl = __popc(lm);
-            for (int k = 0; k < nl; ++k) acc_e -= S.sw[0][k];
             const int npc = __popc(b1) + __popc(b2);
             if (npc) {
                 if (np + npc > kPend && !pend_spill(S, gm, cap, np, gtop, npc)) {
@@ -279,10 +275,10 @@ __device__ void solo_pop(const RoundArgs& a, RoundSmem& S, const StackEntry& c, 
         if (prev >= 0 && lane == 0) a.nx[c.e] = prev;
         if (lane == 0) a.pop_wcnt[c.e] = nl_total;
     }
-    a.rec[c.e].pe = acc_e;
+    // the own perEdge as in the windowed commit: k_pop_pe folds the logged weights
     a.rec[c.e].ss = (s_e - (uint32_t)nl_total) | SS_N;
     if (lane == 0) {
-        if (fabs(acc_e) > a.inv_n) atomicAdd(a.diag, 1ull);
+        if (nl_total == 0 && fabs(pe_e) > a.inv_n) atomicAdd(a.diag, 1ull);
         removed += (unsigned long long)nl_total;
     }
     __syncwarp();
@@ -467,7 +463,7 @@ __global__ void __launch_bounds__(kRoundBlock, 1) k_clean_rounds(RoundArgs a)
         if (active && !lng && lane == ol) mine = so >= 0 && S.hown[so] == (unsigned)wid;
         if (live) mine = mine && s1 >= 0 && s2 >= 0 && S.hown[s1] == (unsigned)wid && S.hown[s2] == (unsigned)wid;
         const bool winner = __all_sync(kFull, mine) && active;
-        double x1 = 0.0, x2 = 0.0, acc_e = ope;
+        double x1 = 0.0, x2 = 0.0;
         bool f1 = false, f2 = false;
         unsigned lm = 0, b1 = 0, b2 = 0;
         if (winner) {
@@ -480,11 +476,6 @@ __global__ void __launch_bounds__(kRoundBlock, 1) k_clean_rounds(RoundArgs a)
             lm = __ballot_sync(kFull, live);
             b1 = __ballot_sync(kFull, f1);
             b2 = __ballot_sync(kFull, f2);
-            if (live) S.sw[wid][__popc(lm & lt)] = t.wgt;
-            __syncwarp();
-            const int nl = __popc(lm);
-#pragma unroll 4
-            for (int k = 0; k < nl; ++k) acc_e -= S.sw[wid][k];
             if (lane == 0 && (b1 | b2)) atomicMin(&ctl.p1, wid);
         } else if (active) {
             if (live) {
@@ -520,12 +511,13 @@ __global__ void __launch_bounds__(kRoundBlock, 1) k_clean_rounds(RoundArgs a)
                 a.wbuf[c.t0 + k] = t.wgt;
                 a.zbuf[c.t0 + k] = t.z;
             }
-            // every lane holds the same values: the same stores from all lanes
-            a.rec[c.e].pe = acc_e;
+            // every lane holds the same values: the same stores from all lanes.  The popped
+            // edge's own perEdge keeps the value it has at the pop; k_pop_pe subtracts the
+            // logged live weights (in triangle order) after the replay, off the round's path.
             a.rec[c.e].ss = (s_e - (uint32_t)nl) | SS_N;
             a.pop_wcnt[c.e] = nl;
             if (lane == 0) {
-                if (fabs(acc_e) > a.inv_n) atomicAdd(a.diag, 1ull);
+                if (nl == 0 && fabs(ope) > a.inv_n) atomicAdd(a.diag, 1ull);
                 removed += (unsigned long long)nl;
                 atomicOr(&ctl.committed, 1u << wid);
             }
@@ -652,6 +644,27 @@ __global__ void k_log_keys(const int32_t* __restrict__ pop_wcnt, const uint32_t*
     }
 }
 
+// perEdge of the edges that k_clean_rounds popped with live triangles: the
+// record kept the value it had at the pop, and the pop's live weights are
+// logged in triangle order at the edge's list offset; they are subtracted now
+// in that order -- the popped edge's own fold in deleteAndClean
+// (RTRex_Sequential/Escape/Decomposition.h:152-281) -- followed by the
+// reference's residual check.  No pop reads a popped edge's perEdge (its
+// triangles are no longer live), so moving the fold here changes no bit.
+__global__ void k_pop_pe(EdgeRec* __restrict__ rec, const int32_t* __restrict__ pop_wcnt,
+                         const double* __restrict__ wbuf, int64_t m, double inv_n, unsigned long long* __restrict__ diag)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t wc = pop_wcnt[e];
+        if (wc <= 0) continue;
+        const int64_t wo = rec[e].t0;
+        double x = rec[e].pe;
+        for (int32_t k = 0; k < wc; ++k) x -= wbuf[wo + k];
+        rec[e].pe = x;
+        if (fabs(x) > inv_n) atomicAdd(diag, 1ull);
+    }
+}
+
 // perVertex of the round-replayed units: the logged subtractions of each
 // vertex in the reference's pop order (within a pop, triangle order).
 __global__ void k_pv_fold(const uint64_t* __restrict__ keys, int64_t cnt, int pb, const int32_t* __restrict__ inv,
@@ -753,6 +766,7 @@ int clean_rounds_finish(rtr_graph* g, Scratch& sc, RoundReplay* rr)
     const int64_t m = g->m, nbig = rr->nbig;
     const int kB = 256;
     const int gb = grid_for(nbig, kB), gm = grid_for(m, kB);
+    k_pop_pe<<<gm, kB, 0, s>>>(rr->rec, rr->pop_wcnt, rr->wbuf, m, 1 / (double)g->n, g->ctr + 2);
     // rank every pop in the reference's order
     k_rank_init<<<gm, kB, 0, s>>>(rr->nx, rr->dd, m);
     const int steps = bits_for((uint64_t)m) + 1;
@@ -769,7 +783,7 @@ int clean_rounds_finish(rtr_graph* g, Scratch& sc, RoundReplay* rr)
     k_round_tails<<<gb, kB, 0, s>>>(rr->units, rr->order, nbig, rr->seeds, rr->nx, rr->len, rr->ubase, tpos);
     k_log_count<<<gm, kB, 0, s>>>(rr->pop_wcnt, m, rr->logcnt);
     exclusive_scan_u32(rr->logcnt, rr->logoff, m, rr->logoff + m, rr->logtmp, s);
-    g->launches += 1 + steps + 4 + 2 * 2;
+    g->launches += 2 + steps + 4 + 2 * 2;
     uint32_t nlog = 0;
     RTR_CUDA_TRY(cudaMemcpyAsync(&nlog, rr->logoff + m, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     RTR_CUDA_TRY(cudaStreamSynchronize(s));
