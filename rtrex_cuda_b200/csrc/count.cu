@@ -31,6 +31,8 @@
 #include "rowsets.cuh"
 #include "rtr_graph.cuh"
 
+#include <memory>
+
 namespace rtr {
 
 namespace {
@@ -134,7 +136,8 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
                        const int32_t* __restrict__ partner, const int32_t* __restrict__ heavy_list,
                        const unsigned* __restrict__ nheavy, int gallop, RowSets rs, uint32_t* __restrict__ sup,
                        int64_t* __restrict__ cnt, int64_t* __restrict__ cgt, double* __restrict__ pe,
-                       unsigned long long* __restrict__ total)
+                       unsigned long long* __restrict__ total, const int64_t* __restrict__ moff,
+                       uint32_t* __restrict__ masks)
 {
     __shared__ double s_w[kHeavyEdgeBlock / 32][32];
     __shared__ int32_t s_z[kHeavyEdgeBlock / 32][128];
@@ -158,6 +161,9 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
             // perEdge: the step's hits, in order, are packed one per lane (ballot ranks), so that one
             // pass of divisions serves all four chunks, and enter the chain by shuffle
             const unsigned lt = (1u << lane) - 1u;
+            // masks: each chunk's hit ballot, for the rows layout's list fill
+            const int64_t mw0 = masks ? moff[h] : 0, mwn = masks ? moff[h + 1] - mw0 : 0;
+            int64_t chunk = 0;
             warp_probe_walk<B>(rs, t, nb, u_short ? u0 : v0, u_short ? u1 : v1, nb[(u_short ? v1 : u1) - 1], lane,
                                [&](const bool (&hit)[B], const int32_t (&x)[B]) {
                                    int tot = 0;
@@ -168,8 +174,10 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock)
                                        above_u += (hit[b] && x[b] > u) ? 1u : 0u;
                                        const unsigned mb = __ballot_sync(0xffffffffu, hit[b]);
                                        if (pe && hit[b]) s_z[wib][tot + __popc(mb & lt)] = x[b];
+                                       if (lane == 0 && chunk + b < mwn) masks[mw0 + chunk + b] = mb;
                                        tot += __popc(mb);
                                    }
+                                   chunk += B;
                                    if (!pe || tot == 0) return;
                                    __syncwarp();
                                    for (int q0 = 0; q0 < tot; q0 += 32) {
@@ -229,6 +237,27 @@ __global__ void k_heavy_keys(const int64_t* __restrict__ off, const int32_t* __r
         const int32_t u = esrc[i], v = nb[i];
         const int32_t w = off[u + 1] - off[u] <= off[v + 1] - off[v] ? v : u;
         keys[h] = ((uint64_t)(uint32_t)k << 32) | (uint64_t)(uint32_t)w;
+    }
+}
+
+// Hit-mask words of each heavy edge: one per 32 elements of its shorter row
+// when the longer row has a hash set (the edges the count walks through one),
+// else none.
+__global__ void k_mask_words(const int64_t* __restrict__ off, const int32_t* __restrict__ esrc,
+                             const int32_t* __restrict__ nb, const int32_t* __restrict__ fwd,
+                             const int32_t* __restrict__ heavy_list, int64_t nh, RowSets rs,
+                             int64_t* __restrict__ words)
+{
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h <= nh; h += (int64_t)gridDim.x * blockDim.x) {
+        if (h == nh) {
+            words[h] = 0;
+            continue;
+        }
+        const int64_t i = fwd[heavy_list[h]];
+        const int32_t u = esrc[i], v = nb[i];
+        const int64_t du = off[u + 1] - off[u], dv = off[v + 1] - off[v];
+        const bool u_short = du <= dv;
+        words[h] = rs_table(rs, u_short ? v : u) >= 0 ? ((u_short ? du : dv) + 31) / 32 : 0;
     }
 }
 
@@ -483,10 +512,49 @@ int count_triangles(rtr_graph* g)
             g->launches += 2 + 3 * ((bits_for((uint64_t)(n > 0 ? n - 1 : 0)) + 7) / 8);
         }
     }
+    // Hit masks of the heavy edges (rows layout possible): the list fill then reads the masks
+    // instead of repeating the lookups.  In their own scratch, released before TriEntry
+    // lists are allocated; skipped when they would take more than a third of the free memory.
+    std::unique_ptr<Scratch> msc;
+    int64_t* moff = nullptr;
+    uint32_t* masks = nullptr;
+    int64_t mask_bytes = 0;
+    if (rs.tab && cgt) {
+        unsigned nh = 0;
+        RTR_CUDA_TRY(cudaMemcpyAsync(&nh, nheavy, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        RTR_CUDA_TRY(cudaStreamSynchronize(s));
+        if (nh > 0) {
+            msc.reset(new Scratch(g));
+            int64_t* wcount = (int64_t*)msc->get(sizeof(int64_t) * (nh + 1));
+            moff = (int64_t*)msc->get(sizeof(int64_t) * (nh + 1));
+            int64_t* wtmp = (int64_t*)msc->get(sizeof(int64_t) * scan_temp_elems(nh + 1));
+            if (!wcount || !moff || !wtmp) {
+                set_error("device allocation failed (hit masks)");
+                return RTR_ERR_CUDA;
+            }
+            k_mask_words<<<grid_for(nh + 1, 256), 256, 0, s>>>(g->offsets, g->esrc, g->nbors, g->fwd, heavy_list,
+                                                                nh, rs, wcount);
+            exclusive_scan_i64(wcount, moff, nh + 1, nullptr, wtmp, s);
+            int64_t words = 0;
+            RTR_CUDA_TRY(cudaMemcpyAsync(&words, moff + nh, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            RTR_CUDA_TRY(cudaStreamSynchronize(s));
+            size_t free_b = 0, total_b = 0;
+            RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+            const int64_t bytes = (int64_t)sizeof(uint32_t) * (words + 1);
+            if (bytes < (int64_t)(free_b / 3)) masks = (uint32_t*)msc->get((size_t)bytes);
+            if (masks) {
+                RTR_CUDA_TRY(cudaMemsetAsync(masks, 0, (size_t)bytes, s));
+                mask_bytes = bytes;
+            } else {
+                moff = nullptr;
+            }
+            g->launches += 2;
+        }
+    }
     ktime_begin(g, KT_EDGE_HEAVY);
     k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd, g->partner,
                                                       heavy_list, nheavy, g->tune_gallop, rs, g->sup, cnt, cgt,
-                                                      heavy_pe ? g->pe : nullptr, g->ctr);
+                                                      heavy_pe ? g->pe : nullptr, g->ctr, moff, masks);
     ktime_end(g, KT_EDGE_HEAVY);
     ktime_end(g, KT_EDGE_FOLD);
     exclusive_scan_i64(cnt, g->tl_off, m2 + 1, nullptr, tmp, s);
@@ -502,7 +570,7 @@ int count_triangles(rtr_graph* g)
         RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
         const double need = (double)sizeof(TriEntry) * (double)(tl_len + 1) + 64.0 * (double)(m + 1) +
                             (double)(1ll << 30);
-        keep_lists = need <= (double)free_b;
+        keep_lists = need <= (double)free_b + (double)mask_bytes;
     }
     if (!keep_lists) {
         // rows layout: perVertex and heavy-edge perEdge straight from the CSR rows
@@ -516,11 +584,11 @@ int count_triangles(rtr_graph* g)
             }
             k_edge_count_heavy<<<gh, kHeavyEdgeBlock, 0, s>>>(g->offsets, g->nbors, g->esrc, g->deg, g->fwd,
                                                               g->partner, heavy_list, nheavy, g->tune_gallop, rs,
-                                                              g->sup, cnt, nullptr, g->pe, junk);
+                                                              g->sup, cnt, nullptr, g->pe, junk, nullptr, nullptr);
             g->launches += 1;
         }
         // cnt (scanned into tl_off above) is free: it takes the lists' offsets
-        const int rc = count_rows(g, sc, rs, cgt, cnt, heavy_list, nheavy);
+        const int rc = count_rows(g, sc, rs, cgt, cnt, heavy_list, nheavy, moff, masks);
         if (rc) return rc;
         RTR_CUDA_TRY(cudaGetLastError());
         cudaEventRecord(e1, s);
@@ -534,6 +602,7 @@ int count_triangles(rtr_graph* g)
         g->stage = 2;
         return RTR_OK;
     }
+    msc.reset();  // the hit masks are for the rows layout only
     if (tl_len > g->tl_len || !g->tl) {
         // grow-only buffer owned by the graph
         g->tl = (TriEntry*)dev_alloc(g, sizeof(TriEntry) * (tl_len + 1));

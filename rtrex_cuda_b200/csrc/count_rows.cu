@@ -61,6 +61,8 @@ struct FillArgs {
     int64_t p0, p1;       // the window's slots
     int64_t e0;           // lpos[p0]: entry e of the window lives at lists[e - e0]
     int32_t* lists;
+    const int64_t* moff;    // heavy edge h's hit masks: masks[moff[h] .. moff[h+1]) (null: none)
+    const uint32_t* masks;  // bit k of word j: element 32j + k of the shorter row is common
 };
 
 __device__ __forceinline__ bool in_window(const FillArgs& a, int64_t p) { return p >= a.p0 && p < a.p1; }
@@ -118,7 +120,25 @@ __global__ void __launch_bounds__(kHeavyBlock) k_fill_heavy(FillArgs a, const in
             qi += __popc(mi);
         };
         const int32_t t = rs_table(a.rs, u_short ? v : u);
-        if (t >= 0) {
+        if (t >= 0 && a.masks) {
+            // the count's hit masks: only chunks with hits are read, no lookups
+            const int64_t w0 = a.moff[h], nw = a.moff[h + 1] - w0;
+            const int64_t sa = u_short ? u0 : v0;  // where the count's walk began
+            for (int64_t cb = (s0 - sa) / 32; cb < nw; cb += 32) {
+                const int64_t cc = cb + lane;
+                const uint32_t mw = cc < nw ? __ldg(a.masks + w0 + cc) : 0u;
+                unsigned nz = __ballot_sync(0xffffffffu, mw != 0u);
+                while (nz) {  // uniform across the warp
+                    const int j = __ffs(nz) - 1;
+                    nz &= nz - 1u;
+                    const uint32_t mj = __shfl_sync(0xffffffffu, mw, j);
+                    const int64_t p = sa + (cb + j) * 32 + lane;
+                    const bool hit = ((mj >> lane) & 1u) && p >= s0;  // before s0: z < from
+                    const int32_t z = hit ? a.nb[p] : 0;
+                    emit(hit, z, hit ? a.deg[z] : 0);
+                }
+            }
+        } else if (t >= 0) {
             constexpr int B = 4;  // 4 chunks per step, their lookups (then degrees) in flight together
             warp_probe_walk<B>(a.rs, t, a.nb, s0, s1, a.nb[(u_short ? v1 : u1) - 1], lane,
                                [&](const bool (&hit)[B], const int32_t (&x)[B]) {
@@ -562,7 +582,7 @@ int build_row_sets(rtr_graph* g, Scratch& sc, int min_deg, RowSets* out)
 // pass (support, total, perEdge of all edges, cgt).  Synchronises the graph's
 // stream.
 int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt, int64_t* lpos,
-               const int32_t* heavy_list, const unsigned* nheavy)
+               const int32_t* heavy_list, const unsigned* nheavy, const int64_t* moff, const uint32_t* masks)
 {
     cudaStream_t s = g->stream;
     const int64_t n = g->n, m2 = g->m2, m = g->m;
@@ -681,7 +701,7 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
             break;
         }
         FillArgs fa{g->offsets, g->nbors, g->esrc, g->partner, g->deg, g->fwd, m, g->tune_edge, g->tune_gallop,
-                    rs, lpos, p01[0], p01[1], e01[0], lists};
+                    rs, lpos, p01[0], p01[1], e01[0], lists, moff, masks};
         ktime_begin(g, KT_TRI_FILL);
         ktime_begin(g, KT_FILL_LIGHT);
         k_fill_light<<<grid_for(m, kFillBlock), kFillBlock, 0, s>>>(fa);

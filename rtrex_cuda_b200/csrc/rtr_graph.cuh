@@ -178,9 +178,10 @@ struct RowSets;
 // hash sets of the rows of at least min_deg entries, in sc (count_rows.cu)
 int build_row_sets(rtr_graph* g, Scratch& sc, int min_deg, RowSets* out);
 // rows layout: perVertex from per-slot lists of z (count_rows.cu); cgt the
-// per-slot term counts, lpos room for their scan, heavy_list the heavy edges
+// per-slot term counts, lpos room for their scan, heavy_list the heavy edges,
+// masks (may be null) the count's hit masks of them at word offsets moff
 int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt, int64_t* lpos,
-               const int32_t* heavy_list, const unsigned* nheavy);
+               const int32_t* heavy_list, const unsigned* nheavy, const int64_t* moff, const uint32_t* masks);
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 int initial_clean(rtr_graph* g, double eps);
 int extract_clusters(rtr_graph* g);
