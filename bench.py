@@ -338,6 +338,7 @@ def rmat24_leg(args, dev, flush_l2, peak, peak_kind, scale=24, steps=None, mode=
         ms.append(g.stats()["ms_count"])
     launches = (g.stats()["launches"] - launches0) // steps
     layout = "rows (no triangle lists)" if not g.count_mode()[2] else "triangle lists"
+    windows, list_entries = g.count_windows()
     kms = g.kernel_ms()
     off, nb = g.csr()
     g.close()
@@ -346,7 +347,8 @@ def rmat24_leg(args, dev, flush_l2, peak, peak_kind, scale=24, steps=None, mode=
     t = float(np.mean(ms)) / 1e3
     out = {"workload": f"rmat{scale}", "desc": f"R-MAT scale {scale}, edge factor 16, a,b,c,d = .57,.19,.19,.05, "
                                                 "seed 3, symmetrised, self-loops and repeats dropped (device generator)",
-           "n": n, "m": m, "triangles": total, "layout": layout, "steps": steps,
+           "n": n, "m": m, "triangles": total, "layout": layout, "list_windows": windows,
+           "list_entries": list_entries, "steps": steps,
            "ms_per_count": t * 1e3, "edges_per_s": m / t, "triangles_per_s": total / t,
            "generation_and_csr_build_ms": gen_ms,
            "kernel_ms": {"edge_fold_and_heavy_count": kms["k_edge_fold"],
@@ -397,7 +399,8 @@ def rmat_count_arm(args):
             "n_gpus": 1, "steps": r["steps"], "warmup": 1, "ms_per_step": r["ms_per_count"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": r["workload"], "desc": r["desc"], "n": r["n"], "m": r["m"],
-                       "layout": r["layout"], "l2": "flushed (256 MiB write) before every step"},
+                       "layout": r["layout"], "list_windows": r["list_windows"],
+                       "l2": "flushed (256 MiB write) before every step"},
             "triangles": r["triangles"], "triangles_per_s": r["triangles_per_s"], "e2e": r.get("e2e"),
             "roofline": r["roofline_count"], "gpu_launches": r["gpu_launches_per_count"] * r["steps"],
             "kernel_ms": r["kernel_ms"], "generation_and_csr_build_ms": r["generation_and_csr_build_ms"]}

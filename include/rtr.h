@@ -133,6 +133,11 @@ int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int
  * (RTRex_Sequential/Escape/Decomposition.h:42-117). */
 int rtr_set_count_mode(rtr_graph* g, int mode, int hub_degree);
 int rtr_get_count_mode(const rtr_graph* g, int* mode, int* hub_degree, int* lists_kept);
+/* Rows layout of the last rtr_count: the windows of whole rows its per-slot
+ * lists were filled and folded in (1 when they all fit in free device memory)
+ * and their total entries (3 per triangle); both 0 when the lists were kept.
+ * No counterpart in the reference. */
+int rtr_get_count_windows(const rtr_graph* g, int64_t* windows, int64_t* list_entries);
 
 /* Split of the cascading clean: units (connected components of the
  * triangle-carrying edges) with at least min_seeds seeds and triangle lists of

@@ -106,6 +106,7 @@ def lib():
     L.rtr_autotune.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rtr_set_count_mode.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.rtr_get_count_mode.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rtr_get_count_windows.argtypes = [_vp, P(ctypes.c_int64), P(ctypes.c_int64)]
     L.rtr_graph_create_rmat.argtypes = [ctypes.c_int, _i64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_uint64, ctypes.c_int, P(_vp)]
     L.rtr_set_clean_split.argtypes = [_vp, _i64, ctypes.c_double]
@@ -360,6 +361,12 @@ class Graph:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(lib().rtr_get_count_mode(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return int(a.value), int(b.value), bool(c.value)
+
+    def count_windows(self):
+        """(windows, list entries) of the last count's rows layout; (0, 0) with lists kept."""
+        w, e = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().rtr_get_count_windows(self._h, ctypes.byref(w), ctypes.byref(e)))
+        return int(w.value), int(e.value)
 
     def set_clean_split(self, min_seeds: int, max_mean_list: float = 8.0):
         """Clean units with at least `min_seeds` seeds and triangle lists of at

@@ -388,6 +388,17 @@ int rtr_get_count_mode(const rtr_graph* g, int* mode, int* hub_degree, int* list
     return RTR_OK;
 }
 
+int rtr_get_count_windows(const rtr_graph* g, int64_t* windows, int64_t* list_entries)
+{
+    if (!g) {
+        set_error("null graph");
+        return RTR_ERR_ARG;
+    }
+    if (windows) *windows = g->lists ? 0 : g->rows_windows;
+    if (list_entries) *list_entries = g->lists ? 0 : g->rows_entries;
+    return RTR_OK;
+}
+
 int rtr_set_clean_split(rtr_graph* g, int64_t min_seeds, double max_mean_list)
 {
     if (!g || min_seeds < 1 || !(max_mean_list >= 0)) {

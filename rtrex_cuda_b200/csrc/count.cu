@@ -538,8 +538,7 @@ int count_triangles(rtr_graph* g)
             int64_t words = 0;
             RTR_CUDA_TRY(cudaMemcpyAsync(&words, moff + nh, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
             RTR_CUDA_TRY(cudaStreamSynchronize(s));
-            size_t free_b = 0, total_b = 0;
-            RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+            const size_t free_b = free_device_bytes(g, true);
             const int64_t bytes = (int64_t)sizeof(uint32_t) * (words + 1);
             if (bytes < (int64_t)(free_b / 3)) masks = (uint32_t*)msc->get((size_t)bytes);
             if (masks) {
@@ -565,9 +564,9 @@ int count_triangles(rtr_graph* g)
     RTR_CUDA_TRY(cudaStreamSynchronize(s));
     bool keep_lists = g->count_mode != 2;
     if (g->count_mode == 0 && (tl_len > g->tl_len || !g->tl)) {
-        // keep the lists only when they fit beside what the clean will need (records, stacks)
-        size_t free_b = 0, total_b = 0;
-        RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        // keep the lists only when they fit beside what the clean will need (records, stacks);
+        // a large graph first has the pool return its cached blocks
+        const size_t free_b = free_device_bytes(g, rs.tab != nullptr);
         const double need = (double)sizeof(TriEntry) * (double)(tl_len + 1) + 64.0 * (double)(m + 1) +
                             (double)(1ll << 30);
         keep_lists = need <= (double)free_b + (double)mask_bytes;

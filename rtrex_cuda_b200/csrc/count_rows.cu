@@ -650,8 +650,7 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         g->launches += 3;
     }
     // the lists: all of them when they fit in the free HBM (less 1 GiB), else windows of whole rows
-    size_t free_b = 0, total_b = 0;
-    RTR_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const size_t free_b = free_device_bytes(g, true);
     const int64_t margin = 1ll << 30;
     const int64_t fit = (int64_t)free_b > margin ? ((int64_t)free_b - margin) / (int64_t)sizeof(int32_t) : 0;
     const int64_t room = want < fit ? want : fit;
@@ -672,7 +671,10 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
     if (nhuge > 0) RTR_CUDA_TRY(cudaFuncSetAttribute(k_vfold_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                      (int)kBlockFoldSmem));
     int rc = RTR_OK;
+    g->rows_windows = 0;
+    g->rows_entries = want;
     for (int64_t x0 = 0; x0 < n && rc == RTR_OK;) {
+        ++g->rows_windows;
         int64_t x1 = n;
         if (want > room) {
             k_window_end<<<1, 1, 0, s>>>(g->offsets, lpos, n, x0, room, d_x1);

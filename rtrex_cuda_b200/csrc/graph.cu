@@ -75,6 +75,23 @@ Scratch::~Scratch()
     g->scratch_bytes -= bytes;
 }
 
+// Free device memory.  The device pool keeps freed blocks cached (its release
+// threshold is unbounded), and cudaMemGetInfo counts them as used; with trim the
+// pool first returns the blocks no allocation holds, so the figure is what a
+// large allocation can get.
+size_t free_device_bytes(rtr_graph* g, bool trim)
+{
+    if (trim) {
+        cudaStreamSynchronize(g->stream);
+        if (g->side) cudaStreamSynchronize(g->side);
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, g->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+    return free_b;
+}
+
 namespace {
 
 constexpr int kBlock = 256;

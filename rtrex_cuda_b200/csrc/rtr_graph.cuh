@@ -86,6 +86,8 @@ struct rtr_graph {
     // 1 always keep them, 2 never (rows layout: folds straight from the CSR);
     // count_hub: perVertex terms from which the rows layout folds a vertex with a warp
     int count_mode = 0;
+    int64_t rows_windows = 0;  // rows layout: windows the last count took, and its list entries
+    int64_t rows_entries = 0;
     int count_hub = 1024;
     bool lists = false;  // the last count kept the triangle lists (the clean needs them)
     // clean units with at least this many seeds and triangle lists of at most
@@ -171,6 +173,8 @@ struct Scratch {
     ~Scratch();
 };
 
+// free device memory; trim: first return the pool's cached blocks (graph.cu)
+size_t free_device_bytes(rtr_graph* g, bool trim);
 int build_csr(rtr_graph* g, const int64_t* d_u, const int64_t* d_v, int64_t m, bool simplify);
 int build_csr_from_host_csr(rtr_graph* g, const int64_t* h_offsets, const int64_t* h_nbors);
 int count_triangles(rtr_graph* g);
