@@ -513,8 +513,8 @@ int count_triangles(rtr_graph* g)
         }
     }
     // Hit masks of the heavy edges (rows layout possible): the list fill then reads the masks
-    // instead of repeating the lookups.  In their own scratch, released before TriEntry
-    // lists are allocated; skipped when they would take more than a third of the free memory.
+    // instead of repeating the lookups.  A graph-owned buffer (reused by later counts);
+    // skipped when it would take more than a third of the free memory.
     std::unique_ptr<Scratch> msc;
     int64_t* moff = nullptr;
     uint32_t* masks = nullptr;
@@ -538,9 +538,11 @@ int count_triangles(rtr_graph* g)
             int64_t words = 0;
             RTR_CUDA_TRY(cudaMemcpyAsync(&words, moff + nh, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
             RTR_CUDA_TRY(cudaStreamSynchronize(s));
-            const size_t free_b = free_device_bytes(g, true);
             const int64_t bytes = (int64_t)sizeof(uint32_t) * (words + 1);
-            if (bytes < (int64_t)(free_b / 3)) masks = (uint32_t*)msc->get((size_t)bytes);
+            if (g->rows_masks_cap >= bytes)
+                masks = (uint32_t*)g->rows_masks;
+            else if (bytes < (int64_t)((device_avail_bytes(g) + g->rows_masks_cap) / 3))
+                masks = (uint32_t*)grow_owned(g, &g->rows_masks, &g->rows_masks_cap, bytes);
             if (masks) {
                 RTR_CUDA_TRY(cudaMemsetAsync(masks, 0, (size_t)bytes, s));
                 mask_bytes = bytes;
@@ -566,10 +568,10 @@ int count_triangles(rtr_graph* g)
     if (g->count_mode == 0 && (tl_len > g->tl_len || !g->tl)) {
         // keep the lists only when they fit beside what the clean will need (records, stacks);
         // a large graph first has the pool return its cached blocks
-        const size_t free_b = free_device_bytes(g, rs.tab != nullptr);
+        const size_t free_b = device_avail_bytes(g) + (size_t)g->rows_masks_cap + (size_t)g->rows_lists_cap;
         const double need = (double)sizeof(TriEntry) * (double)(tl_len + 1) + 64.0 * (double)(m + 1) +
                             (double)(1ll << 30);
-        keep_lists = need <= (double)free_b + (double)mask_bytes;
+        keep_lists = need <= (double)free_b;
     }
     if (!keep_lists) {
         // rows layout: perVertex and heavy-edge perEdge straight from the CSR rows
@@ -601,7 +603,10 @@ int count_triangles(rtr_graph* g)
         g->stage = 2;
         return RTR_OK;
     }
-    msc.reset();  // the hit masks are for the rows layout only
+    msc.reset();
+    // the rows layout's buffers are not needed with lists
+    release_owned(g, &g->rows_masks, &g->rows_masks_cap);
+    release_owned(g, &g->rows_lists, &g->rows_lists_cap);
     if (tl_len > g->tl_len || !g->tl) {
         // grow-only buffer owned by the graph
         g->tl = (TriEntry*)dev_alloc(g, sizeof(TriEntry) * (tl_len + 1));

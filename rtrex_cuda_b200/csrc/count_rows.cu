@@ -649,12 +649,26 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         k_seg_slots<<<grid_for(1ll << 40, 256, 4), 256, 0, s>>>(g->offsets, lpos, big, nhuge, segoff, segslot);
         g->launches += 3;
     }
-    // the lists: all of them when they fit in the free HBM (less 1 GiB), else windows of whole rows
-    const size_t free_b = free_device_bytes(g, true);
+    // the lists: all of them when they fit in the free HBM (less 1 GiB), else windows of whole
+    // rows; a graph-owned buffer, reused by later counts of the graph
     const int64_t margin = 1ll << 30;
-    const int64_t fit = (int64_t)free_b > margin ? ((int64_t)free_b - margin) / (int64_t)sizeof(int32_t) : 0;
-    const int64_t room = want < fit ? want : fit;
-    int32_t* lists = (int32_t*)sc.get(sizeof(int32_t) * (room + 1));
+    int64_t room = 0;
+    int32_t* lists = nullptr;
+    if (g->rows_lists_cap >= (int64_t)sizeof(int32_t) * (want + 1)) {
+        room = want;
+        lists = (int32_t*)g->rows_lists;
+    } else {
+        const int64_t avail = (int64_t)device_avail_bytes(g) + g->rows_lists_cap;
+        const int64_t fit = avail > margin ? (avail - margin) / (int64_t)sizeof(int32_t) - 1 : 0;
+        room = want < fit ? want : fit;
+        // the estimate counts the pool's cached blocks; halve until an allocation succeeds
+        for (int attempt = 0; attempt < 8 && !lists && room >= 0; ++attempt) {
+            lists = (int32_t*)grow_owned(g, &g->rows_lists, &g->rows_lists_cap,
+                                         (int64_t)sizeof(int32_t) * (room + 1));
+            if (!lists) room /= 2;
+        }
+        cudaGetLastError();  // a failed attempt's allocation error is not the caller's
+    }
     if (!lists) {
         set_error("device allocation failed (rows layout: %lld list entries)", (long long)(room + 1));
         return RTR_ERR_CUDA;

@@ -79,6 +79,43 @@ Scratch::~Scratch()
 // threshold is unbounded), and cudaMemGetInfo counts them as used; with trim the
 // pool first returns the blocks no allocation holds, so the figure is what a
 // large allocation can get.
+size_t device_avail_bytes(rtr_graph* g)
+{
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+    cudaMemPool_t pool;
+    uint64_t reserved = 0, used = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, g->device) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+        free_b += (size_t)(reserved - used);
+    return free_b;
+}
+
+void release_owned(rtr_graph* g, void** buf, int64_t* cap)
+{
+    if (!*buf) return;
+    for (size_t k = 0; k < g->owned.size(); ++k)
+        if (g->owned[k] == *buf) {
+            g->owned.erase(g->owned.begin() + (long)k);
+            break;
+        }
+    cudaFreeAsync(*buf, g->stream);
+    g->owned_bytes -= *cap;
+    *buf = nullptr;
+    *cap = 0;
+}
+
+void* grow_owned(rtr_graph* g, void** buf, int64_t* cap, int64_t bytes)
+{
+    if (*cap >= bytes && *buf) return *buf;
+    release_owned(g, buf, cap);
+    free_device_bytes(g, true);  // return the pool's cached blocks first
+    *buf = dev_alloc(g, (size_t)bytes);
+    if (*buf) *cap = bytes;
+    return *buf;
+}
+
 size_t free_device_bytes(rtr_graph* g, bool trim)
 {
     if (trim) {

@@ -88,6 +88,11 @@ struct rtr_graph {
     int count_mode = 0;
     int64_t rows_windows = 0;  // rows layout: windows the last count took, and its list entries
     int64_t rows_entries = 0;
+    // rows layout buffers, owned by the graph and reused by later counts (grow-only)
+    void* rows_masks = nullptr;
+    int64_t rows_masks_cap = 0;
+    void* rows_lists = nullptr;
+    int64_t rows_lists_cap = 0;
     int count_hub = 1024;
     bool lists = false;  // the last count kept the triangle lists (the clean needs them)
     // clean units with at least this many seeds and triangle lists of at most
@@ -175,6 +180,11 @@ struct Scratch {
 
 // free device memory; trim: first return the pool's cached blocks (graph.cu)
 size_t free_device_bytes(rtr_graph* g, bool trim);
+// free device memory plus the pool's cached blocks, without trimming
+size_t device_avail_bytes(rtr_graph* g);
+// a graph-owned grow-only buffer of at least `bytes` (trims the pool before growing; null on failure)
+void* grow_owned(rtr_graph* g, void** buf, int64_t* cap, int64_t bytes);
+void release_owned(rtr_graph* g, void** buf, int64_t* cap);
 int build_csr(rtr_graph* g, const int64_t* d_u, const int64_t* d_v, int64_t m, bool simplify);
 int build_csr_from_host_csr(rtr_graph* g, const int64_t* h_offsets, const int64_t* h_nbors);
 int count_triangles(rtr_graph* g);
