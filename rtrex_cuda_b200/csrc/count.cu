@@ -130,7 +130,7 @@ constexpr int kHeavyEdgeBlock = 128;
 // pe (may be null): also fold perEdge of the heavy edges, in ascending z, from
 // an ordered walk of the shorter row (the lists layout folds them from the
 // lists instead, k_pe_fold_heavy).  cgt as in k_edge_fold.
-__global__ void __launch_bounds__(kHeavyEdgeBlock)
+__global__ void __launch_bounds__(kHeavyEdgeBlock, 6)
     k_edge_count_heavy(const int64_t* __restrict__ off, const int32_t* __restrict__ nb, const int32_t* __restrict__ esrc,
                        const int32_t* __restrict__ deg, const int32_t* __restrict__ fwd,
                        const int32_t* __restrict__ partner, const int32_t* __restrict__ heavy_list,

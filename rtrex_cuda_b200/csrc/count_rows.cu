@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(kFillBlock) k_fill_light(FillArgs a)
 }
 
 // Heavy edges, a warp each, from the count's heavy-edge list.
-__global__ void __launch_bounds__(kHeavyBlock) k_fill_heavy(FillArgs a, const int32_t* __restrict__ heavy_list,
+__global__ void __launch_bounds__(kHeavyBlock, 8) k_fill_heavy(FillArgs a, const int32_t* __restrict__ heavy_list,
                                                              const unsigned* __restrict__ nheavy)
 {
     const int lane = threadIdx.x & 31;
