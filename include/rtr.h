@@ -138,6 +138,12 @@ int rtr_get_count_mode(const rtr_graph* g, int* mode, int* hub_degree, int* list
  * and their total entries (3 per triangle); both 0 when the lists were kept.
  * No counterpart in the reference. */
 int rtr_get_count_windows(const rtr_graph* g, int64_t* windows, int64_t* list_entries);
+/* At most max_entries per-slot list entries per rows-layout window (0, the
+ * default: as many as fit in free device memory).  Results are the same bits
+ * for every setting; smaller windows only take more passes (a vertex whose
+ * perVertex terms exceed the window is an RTR_ERR_LIMIT).  No counterpart in
+ * the reference. */
+int rtr_set_count_window(rtr_graph* g, int64_t max_entries);
 
 /* Split of the cascading clean: units (connected components of the
  * triangle-carrying edges) with at least min_seeds seeds and triangle lists of

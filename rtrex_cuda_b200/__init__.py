@@ -107,6 +107,7 @@ def lib():
     L.rtr_set_count_mode.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.rtr_get_count_mode.argtypes = [_vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rtr_get_count_windows.argtypes = [_vp, P(ctypes.c_int64), P(ctypes.c_int64)]
+    L.rtr_set_count_window.argtypes = [_vp, ctypes.c_int64]
     L.rtr_graph_create_rmat.argtypes = [ctypes.c_int, _i64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_uint64, ctypes.c_int, P(_vp)]
     L.rtr_set_clean_split.argtypes = [_vp, _i64, ctypes.c_double]
@@ -361,6 +362,10 @@ class Graph:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(lib().rtr_get_count_mode(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return int(a.value), int(b.value), bool(c.value)
+
+    def set_count_window(self, max_entries: int):
+        """Rows layout: at most max_entries list entries per window (0: as many as fit)."""
+        _check(lib().rtr_set_count_window(self._h, int(max_entries)))
 
     def count_windows(self):
         """(windows, list entries) of the last count's rows layout; (0, 0) with lists kept."""

@@ -388,6 +388,16 @@ int rtr_get_count_mode(const rtr_graph* g, int* mode, int* hub_degree, int* list
     return RTR_OK;
 }
 
+int rtr_set_count_window(rtr_graph* g, int64_t max_entries)
+{
+    if (!g || max_entries < 0) {
+        set_error("rtr_set_count_window: null graph or negative entry count");
+        return RTR_ERR_ARG;
+    }
+    g->rows_window_cap = max_entries;
+    return RTR_OK;
+}
+
 int rtr_get_count_windows(const rtr_graph* g, int64_t* windows, int64_t* list_entries)
 {
     if (!g) {

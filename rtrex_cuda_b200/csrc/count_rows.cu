@@ -673,6 +673,7 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
         set_error("device allocation failed (rows layout: %lld list entries)", (long long)(room + 1));
         return RTR_ERR_CUDA;
     }
+    if (g->rows_window_cap > 0 && room > g->rows_window_cap) room = g->rows_window_cap;
     if (!g->side) RTR_CUDA_TRY(cudaStreamCreateWithFlags(&g->side, cudaStreamNonBlocking));
     cudaEvent_t ready = nullptr, joined = nullptr;
     RTR_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));

@@ -86,6 +86,7 @@ struct rtr_graph {
     // 1 always keep them, 2 never (rows layout: folds straight from the CSR);
     // count_hub: perVertex terms from which the rows layout folds a vertex with a warp
     int count_mode = 0;
+    int64_t rows_window_cap = 0;  // rows layout: list entries per window at most (0: as many as fit)
     int64_t rows_windows = 0;  // rows layout: windows the last count took, and its list entries
     int64_t rows_entries = 0;
     // rows layout buffers, owned by the graph and reused by later counts (grow-only)

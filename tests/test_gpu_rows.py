@@ -60,6 +60,33 @@ def test_rows_layout_bit_exact(name):
         assert (sup == s0.support).all(), (name, split)
 
 
+@pytest.mark.parametrize("name", ["chung_lu", "rmat14", "clean_astro"])
+def test_rows_layout_in_windows_bit_exact(name):
+    """Per-slot lists taken in several windows of whole rows (as at R-MAT scale 24,
+    where they do not fit in one): the same bits as the oracle."""
+    (_, _, _), c, s0, _, _, _ = helpers.oracle_run(name, 0.3)
+    n, u, v = helpers.case_graph(name)
+    with rtr.Graph.from_edges(n, u, v) as g:
+        g.set_count_mode(2)
+        assert g.count() == s0.total
+        windows, entries = g.count_windows()
+        assert windows == 1 and entries == 3 * s0.total
+        g.set_count_window(max(entries // 5, 1))  # a window must hold the largest vertex's terms
+        try:
+            total = g.count()
+        except rtr.RtrError as e:  # one vertex alone above the window: pick a larger one
+            assert e.code == 4 and "alone has" in str(e)
+            g.set_count_window(entries // 2)
+            total = g.count()
+        assert total == s0.total
+        windows, _ = g.count_windows()
+        assert windows > 1, (name, windows)
+        pe, pv, sup, _ = g.weights()
+        assert (helpers.bits(pe) == helpers.bits(s0.perEdge)).all()
+        assert (helpers.bits(pv) == helpers.bits(s0.perVertex)).all()
+        assert (sup == s0.support).all()
+
+
 def test_rows_layout_then_lists_again():
     n, u, v = helpers.case_graph("sbm_3000_4002")
     (_, _, _), c, s0, s1, _, _ = helpers.oracle_run("sbm_3000_4002", 0.1)
