@@ -21,6 +21,15 @@
 //                  per light vertex, a warp per heavy one
 //   k_edge_count_heavy / k_tri_fill_heavy / k_pe_fold_heavy  the same for edges
 //                  with deg u + deg v >= g->tune_edge, one warp per edge
+// On large graphs (2m >= 2^25, or the rows layout forced) the rows of at least
+// 256 entries get hash sets first (rowsets.cuh); an intersection whose longer
+// row has one walks the shorter row against it (a warp per heavy edge four
+// chunks of 32 per step, the heavy edges in the order of the sets they probe,
+// so that the probed sets stay in L2).  The same pass also counts, for both
+// slots of every edge, the common neighbours above the slot's neighbour (the
+// rows layout's per-slot term counts, count_rows.cu), folds the heavy edges'
+// perEdge in z order, and records each heavy edge's per-chunk hit masks for the
+// rows layout's list fill.
 // Three work-split parameters (g->tune_gallop: the row-length ratio above which
 // an intersection gallops instead of merging; g->tune_heavy: the degree from
 // which a vertex is folded by a warp; g->tune_edge: the degree sum from which an

@@ -18,21 +18,27 @@
 //             entry holds deg z, all that the fold needs of z.
 //             Slots are taken in windows of whole rows that fit in the free
 //             HBM (one window when everything fits).
-//   fill      one more intersection per edge (u < v) restricted to z > u
-//             writes both slots' lists in ascending z: deg z for z > u to slot
-//             (v,u), for z > v to slot (u,v).  k_fill_light: a thread per light edge;
-//             k_fill_heavy: a warp per heavy edge, hits ranked by ballot.
+//   fill      one more pass per edge (u < v), restricted to z > u, writes
+//             both slots' lists in ascending z: deg z for z > u to slot (v,u),
+//             for z > v to slot (u,v).  k_fill_light: a thread per light edge
+//             (the intersection again); k_fill_heavy: a warp per heavy edge,
+//             which reads the count's hit masks (one 32-bit word per 32
+//             elements of the shorter row) instead of repeating the lookups,
+//             hits ranked by ballot.
 //   fold      perVertex[x] = the left fold of x's slots' lists in slot order
 //             (y ascending), each in z order -- exactly commonNbr's order.
-//             k_vfold_thread: a thread per vertex of few terms;
-//             k_vfold_warp: a warp per vertex of at least `warp_min` terms,
-//             vertices dealt from a queue in descending term count, the
-//             weights of 32 terms computed by the lanes and added in lane
-//             order (the one sequential part: ~10^8 adds for the largest
-//             R-MAT scale-24 hub), with the terms and their degrees loaded
-//             blocks ahead of the add chain.
+//             k_vfold_thread: a thread per vertex of fewer than warp_min terms;
+//             k_vfold_warp: a warp per vertex of fewer than 64 x warp_min, the
+//             weights of 32 terms computed by the lanes (each term's slot by a
+//             shuffle search over 32 slot ends) and added in lane order;
+//             k_vfold_block: a thread block per larger vertex, seven warps
+//             producing weights into shared memory and one warp running the
+//             add chain -- the one sequential part (~10^8 dependent adds for
+//             the largest R-MAT scale-24 vertex).  Vertices are dealt from
+//             queues in descending term count.
 // Membership lookups use the hash sets of the long rows (rowsets.cuh,
-// build_row_sets below).
+// build_row_sets below).  The lists (and the hit masks) are graph-owned
+// buffers that later counts reuse.
 #include "intersect.cuh"
 #include "primitives.cuh"
 #include "rowsets.cuh"
