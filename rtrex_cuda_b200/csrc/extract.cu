@@ -188,8 +188,12 @@ struct Cand {
     double wgt;
 };
 
+// A deletion-stack entry: the edge, the endpoint it was pushed from, the other
+// endpoint, and its triangle list (offset, length), so that a pop's first
+// entries are loaded together with its records.
 struct DelEntry {
-    int32_t e, first, second, pad;
+    int32_t e, first, second, cnt;
+    int64_t t0;
 };
 
 struct ExtractArgs {
@@ -245,6 +249,9 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
         __syncwarp();  // pushes and stores of the previous pop are visible
         const DelEntry d = stack[--top];
         const int32_t e = d.e, u = d.first, v = d.second;
+        // the first 32 entries, issued with the edge's own records
+        TriEntry t_first{};
+        if (lane < d.cnt) t_first = a.tl[d.t0 + lane];
         const uint32_t s_e = a.sup[e];
         if (s_e == 0) {
             if (lane == 0) {
@@ -262,13 +269,14 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
         const bool lower_is_a = lower == a.esrc[e];
         double acc_e = a.pe[e], acc_u = a.pv[u], acc_v = a.pv[v];
         uint32_t rem = 0;
-        const int64_t p1end = a.tl_off[e + 1];
+        const int64_t p1end = d.t0 + d.cnt;
         bool overflow = false;
-        for (int64_t pb = a.tl_off[e]; pb < p1end; pb += 32) {
+        for (int64_t pb = d.t0; pb < p1end; pb += 32) {
             const int64_t p = pb + lane;
             const bool valid = p < p1end;
             TriEntry t{};
-            if (valid) t = a.tl[p];
+            if (pb == d.t0) t = t_first;
+            else if (valid) t = a.tl[p];
             const int32_t elw = lower_is_a ? t.eaz : t.ebz;
             const int32_t ehw = lower_is_a ? t.ebz : t.eaz;
             // statuses, weights and supports of the triangle's other cells in one
@@ -276,6 +284,7 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
             uint8_t slw = ST_N, shw = ST_N;
             double pel = 0.0, peh = 0.0, pz = 0.0;
             uint32_t sul = 0, suh = 0;
+            int64_t tlw0 = 0, tlw1 = 0, thw0 = 0, thw1 = 0;  // their lists, for a push
             if (valid) {
                 slw = a.st[elw];
                 shw = a.st[ehw];
@@ -284,6 +293,10 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
                 pz = a.pv[t.z];
                 sul = a.sup[elw];
                 suh = a.sup[ehw];
+                tlw0 = a.tl_off[elw];
+                tlw1 = a.tl_off[elw + 1];
+                thw0 = a.tl_off[ehw];
+                thw1 = a.tl_off[ehw + 1];
             }
             const bool live = valid && slw != ST_N && shw != ST_N;
             const double wgt = live ? t.wgt : 0.0;
@@ -321,11 +334,11 @@ __device__ void delete_and_clean_warp(const ExtractArgs& a, DelEntry* stack, int
             }
             const int64_t before = top + __popc(b1 & lt) + __popc(b2 & lt);
             if (q1) {
-                stack[before] = DelEntry{elw, lower, t.z, 0};
+                stack[before] = DelEntry{elw, lower, t.z, (int32_t)(tlw1 - tlw0), tlw0};
                 a.st[elw] = ST_S;
             }
             if (q2) {
-                stack[before + (q1 ? 1 : 0)] = DelEntry{ehw, higher, t.z, 0};
+                stack[before + (q1 ? 1 : 0)] = DelEntry{ehw, higher, t.z, (int32_t)(thw1 - thw0), thw0};
                 a.st[ehw] = ST_S;
             }
             top += np;
@@ -584,7 +597,8 @@ __device__ void seed_delete(const ExtractArgs& a, CompCtx& cc, int32_t nm, int64
                 break;
             }
             if (push) {
-                cc.dstack[top + __popc(pm & lt)] = DelEntry{(int32_t)f, z, a.nb[j], 0};
+                const int64_t t0 = a.tl_off[f];
+                cc.dstack[top + __popc(pm & lt)] = DelEntry{(int32_t)f, z, a.nb[j], (int32_t)(a.tl_off[f + 1] - t0), t0};
                 a.st[f] = ST_S;
             }
             top += np;
