@@ -126,8 +126,10 @@ int rtr_get_tuning(const rtr_graph* g, int* gallop_ratio, int* heavy_degree, int
  * of perVertex instead (taken in windows of whole rows when even those do not
  * fit) and folds perVertex from them -- the same bits; a vertex of at least
  * hub_degree perVertex terms (default 1024) is folded by a warp, the others by
- * a thread.  The clean and the extraction need the triangle lists, so
- * rtr_clean then returns
+ * a thread.  Those lists (and, on large graphs, the heavy edges' hit masks)
+ * stay allocated with the graph for its next count, until a count keeps the
+ * triangle lists or rtr_graph_destroy.  The clean and the extraction need the
+ * triangle lists, so rtr_clean then returns
  * RTR_ERR_LIMIT.  *lists_kept tells whether the last rtr_count kept them.  No
  * counterpart in the reference, whose commonNbr keeps no lists
  * (RTRex_Sequential/Escape/Decomposition.h:42-117). */

@@ -527,7 +527,6 @@ int count_triangles(rtr_graph* g)
     std::unique_ptr<Scratch> msc;
     int64_t* moff = nullptr;
     uint32_t* masks = nullptr;
-    int64_t mask_bytes = 0;
     if (rs.tab && cgt) {
         unsigned nh = 0;
         RTR_CUDA_TRY(cudaMemcpyAsync(&nh, nheavy, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -554,7 +553,6 @@ int count_triangles(rtr_graph* g)
                 masks = (uint32_t*)grow_owned(g, &g->rows_masks, &g->rows_masks_cap, bytes);
             if (masks) {
                 RTR_CUDA_TRY(cudaMemsetAsync(masks, 0, (size_t)bytes, s));
-                mask_bytes = bytes;
             } else {
                 moff = nullptr;
             }
