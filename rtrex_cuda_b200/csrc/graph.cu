@@ -110,8 +110,12 @@ void* grow_owned(rtr_graph* g, void** buf, int64_t* cap, int64_t bytes)
 {
     if (*cap >= bytes && *buf) return *buf;
     release_owned(g, buf, cap);
-    free_device_bytes(g, true);  // return the pool's cached blocks first
-    *buf = dev_alloc(g, (size_t)bytes);
+    *buf = dev_alloc(g, (size_t)bytes);  // from the pool's cached blocks when they can serve it
+    if (!*buf) {
+        cudaGetLastError();          // the failed attempt's error is not the caller's
+        free_device_bytes(g, true);  // return the cached blocks, then map fresh memory
+        *buf = dev_alloc(g, (size_t)bytes);
+    }
     if (*buf) *cap = bytes;
     return *buf;
 }
