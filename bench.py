@@ -678,6 +678,7 @@ def ours_arm(args):
         for key, fn in (("config3_rmat24_count",
                          lambda: rmat24_leg(args, dev, flush_l2, peak, peak_kind, steps=1, e2e_runs=1)),
                         ("batched", lambda: batched_leg(args, dev)),
+                        ("served", lambda: served_leg(args, dev)),
                         ("gpu_baseline", lambda: gpu_baseline_leg(dev))):
             try:
                 extras[key] = fn()
@@ -773,11 +774,32 @@ def serve_arm(args):
     plain form on the same request list: one graph at a time, built from host
     arrays and decomposed, no overlap.  Every served result is compared with the
     plain one (clusters, triangle counts, cluster of every vertex)."""
+    world, rank, dev = dist_init()
+    line = serve_run(args, world, rank, dev)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def served_leg(args, dev):
+    """A short served run for the default line (one GPU): 80 requests at 2,000/s
+    over 16 resident graphs of 1K-200K edges, against the plain form."""
+    import copy
+    a = copy.copy(args)
+    a.serve_requests, a.serve_pool, a.serve_max_edges = 80, 16, 2e5
+    line = serve_run(a, 1, 0, dev)
+    keep = ("p50_ms", "p99_ms", "service_p50_ms", "service_p99_ms", "throughput_req_s", "plain",
+            "served_vs_plain_throughput", "results_differing_from_plain")
+    out = {k: line[k] for k in keep}
+    out["config"] = {k: line["config"][k] for k in ("requests", "arrival_rate_per_s", "pool_graphs", "edge_range")}
+    return out
+
+
+def serve_run(args, world, rank, dev):
+    """The served and plain legs of serve_arm; the result line on rank 0 (None elsewhere)."""
     import hashlib
     import torch
     import rtrex_cuda_b200 as rtr
     from rtrex_cuda_b200 import graphgen
-    world, rank, dev = dist_init()
     allmax = lambda x: replica_max(x, world, torch.device("cuda", dev))
     t0 = time.perf_counter()
     pool = graphgen.served_pool(args.serve_pool, m_hi=args.serve_max_edges)
@@ -837,7 +859,7 @@ def serve_arm(args):
     st = {k: sum(d[k] for d in every_st) for k in st}
     edges = int(sum(pool[g][1].size for g in all_graph.tolist()))
     if rank != 0:
-        return
+        return None
     line = {
         "metric": "served p99 latency (ms)", "value": float(np.percentile(lat, 99)), "unit": "ms",
         "n_gpus": world, "steps": N, "warmup": 2, "ms_per_step": float(span_ms / N), "higher_is_better": False,
@@ -858,7 +880,7 @@ def serve_arm(args):
         "results_differing_from_plain": bad, "server_stats": st, "generation_s": gen_s,
         "edges_requested": edges,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
