@@ -575,9 +575,9 @@ int count_triangles(rtr_graph* g)
     if (g->count_mode == 0 && (tl_len > g->tl_len || !g->tl)) {
         // keep the lists only when they fit beside what the clean will need (records, stacks);
         // a large graph first has the pool return its cached blocks
-        // a large graph also counts the pool's cached blocks and its own rows-layout buffers
-        const size_t free_b = rs.tab ? device_avail_bytes(g) + (size_t)g->rows_masks_cap + (size_t)g->rows_lists_cap
-                                     : free_device_bytes(g, false);
+        // free memory counts the pool's cached blocks (an earlier graph's freed buffers, which a
+        // later allocation reuses) and this graph's own rows-layout buffers
+        const size_t free_b = device_avail_bytes(g) + (size_t)g->rows_masks_cap + (size_t)g->rows_lists_cap;
         const double need = (double)sizeof(TriEntry) * (double)(tl_len + 1) + 64.0 * (double)(m + 1) +
                             (double)(1ll << 30);
         keep_lists = need <= (double)free_b;
