@@ -135,13 +135,34 @@ __global__ void __launch_bounds__(kHeavyBlock, 8) k_fill_heavy(FillArgs a, const
                 const uint32_t mw = cc < nw ? __ldg(a.masks + w0 + cc) : 0u;
                 unsigned nz = __ballot_sync(0xffffffffu, mw != 0u);
                 while (nz) {  // uniform across the warp
-                    const int j = __ffs(nz) - 1;
-                    nz &= nz - 1u;
-                    const uint32_t mj = __shfl_sync(0xffffffffu, mw, j);
-                    const int64_t p = sa + (cb + j) * 32 + lane;
-                    const bool hit = ((mj >> lane) & 1u) && p >= s0;  // before s0: z < from
-                    const int32_t z = hit ? a.nb[p] : 0;
-                    emit(hit, z, hit ? a.deg[z] : 0);
+                    // up to four chunks with hits at a time: their element loads, then their
+                    // degree loads, in flight together; emitted in chunk order
+                    constexpr int Q = 4;
+                    int js[Q];
+                    uint32_t ms[Q];
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) {
+                        js[q] = -1;
+                        ms[q] = 0u;
+                        if (nz) {
+                            js[q] = __ffs(nz) - 1;
+                            nz &= nz - 1u;
+                            ms[q] = __shfl_sync(0xffffffffu, mw, js[q]);
+                        }
+                    }
+                    bool hit[Q];
+                    int32_t z[Q], dz[Q];
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) {
+                        const int64_t p = sa + (cb + js[q]) * 32 + lane;
+                        hit[q] = js[q] >= 0 && ((ms[q] >> lane) & 1u) && p >= s0;  // before s0: z < from
+                        z[q] = hit[q] ? a.nb[p] : 0;
+                    }
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) dz[q] = hit[q] ? a.deg[z[q]] : 0;
+#pragma unroll
+                    for (int q = 0; q < Q; ++q)
+                        if (js[q] >= 0) emit(hit[q], z[q], dz[q]);
                 }
             }
         } else if (t >= 0) {
