@@ -149,3 +149,13 @@ def test_clean_split_entry_points_argument_errors():
     k, x = ctypes.c_int64(), ctypes.c_double()
     assert L.rtr_set_clean_split(None, 2048, 8.0) == 1
     assert L.rtr_get_clean_split(None, ctypes.byref(k), ctypes.byref(x)) == 1
+
+
+def test_count_layout_entry_points_argument_errors():
+    L = rtr.lib()
+    a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    w, e = ctypes.c_int64(), ctypes.c_int64()
+    assert L.rtr_set_count_mode(None, 2, 1024) == 1
+    assert L.rtr_get_count_mode(None, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)) == 1
+    assert L.rtr_set_count_window(None, 1000) == 1
+    assert L.rtr_get_count_windows(None, ctypes.byref(w), ctypes.byref(e)) == 1
