@@ -164,21 +164,7 @@ __global__ void __launch_bounds__(kHeavyEdgeBlock, 6)
         const int32_t t = rs_table(rs, u_short ? v : u);
         const int64_t duv = (int64_t)deg[u] * (int64_t)deg[v];
         double acc = 0.0;
-        const int64_t ls = u_short ? u1 - u0 : v1 - v0, ll = u_short ? v1 - v0 : u1 - u0;
-        if (masks && t >= 0 && ll < 2 * ls) {
-            // a balanced pair (the longer row under twice the shorter), with the hit masks kept:
-            // merged by the warp, the rows cut into 32 pieces (sequential reads instead of one
-            // lookup per element) -- counts and hit masks only; its perEdge is folded from the
-            // masks, in z order, by the rows layout's fill (k_fill_heavy)
-            const int64_t mw0 = moff[h], sa = u_short ? u0 : v0;
-            warp_intersect_part(nb, u0, u1, v0, v1, gallop, lane, [&](int32_t z, int64_t pa, int64_t pb) {
-                ++c;
-                above += (z > v) ? 1u : 0u;
-                above_u += (z > u) ? 1u : 0u;
-                const int64_t ps = (u_short ? pa : pb) - sa;
-                atomicOr(&masks[mw0 + (ps >> 5)], 1u << (ps & 31));
-            });
-        } else if (t >= 0) {
+        if (t >= 0) {
             // 4 chunks per step, their lookups and then their degrees in flight together
             constexpr int B = 4;
             // perEdge: the step's hits, in order, are packed one per lane (ballot ranks), so that one

@@ -69,7 +69,6 @@ struct FillArgs {
     int32_t* lists;
     const int64_t* moff;    // heavy edge h's hit masks: masks[moff[h] .. moff[h+1]) (null: none)
     const uint32_t* masks;  // bit k of word j: element 32j + k of the shorter row is common
-    double* pe;             // perEdge, folded here for the balanced pairs the count merged
 };
 
 __device__ __forceinline__ bool in_window(const FillArgs& a, int64_t p) { return p >= a.p0 && p < a.p1; }
@@ -99,12 +98,11 @@ __global__ void __launch_bounds__(kFillBlock) k_fill_light(FillArgs a)
 __global__ void __launch_bounds__(kHeavyBlock, 8) k_fill_heavy(FillArgs a, const int32_t* __restrict__ heavy_list,
                                                              const unsigned* __restrict__ nheavy)
 {
-    __shared__ double s_w[kHeavyBlock / 32][32];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int64_t nh = *nheavy;
     const int64_t nwarps = (int64_t)gridDim.x * (kHeavyBlock / 32);
-    for (int64_t h = (int64_t)blockIdx.x * (kHeavyBlock / 32) + wib; h < nh; h += nwarps) {
+    for (int64_t h = (int64_t)blockIdx.x * (kHeavyBlock / 32) + (threadIdx.x >> 5); h < nh; h += nwarps) {
         const int64_t i = a.fwd[heavy_list[h]];
         const int32_t u = a.esrc[i], v = a.nb[i];
         const int64_t r = a.partner[i];
@@ -129,16 +127,10 @@ __global__ void __launch_bounds__(kHeavyBlock, 8) k_fill_heavy(FillArgs a, const
         };
         const int32_t t = rs_table(a.rs, u_short ? v : u);
         if (t >= 0 && a.masks) {
-            // the count's hit masks: only chunks with hits are read, no lookups.  A balanced pair
-            // (merged by the count, which left its perEdge) also has its perEdge folded here, over
-            // all its hits in z order, in the window that holds its forward slot.
+            // the count's hit masks: only chunks with hits are read, no lookups
             const int64_t w0 = a.moff[h], nw = a.moff[h + 1] - w0;
             const int64_t sa = u_short ? u0 : v0;  // where the count's walk began
-            const int64_t ls = u_short ? u1 - u0 : v1 - v0, ll = u_short ? v1 - v0 : u1 - u0;
-            const bool fold = wi && ll < 2 * ls;
-            const int64_t duv = (int64_t)a.deg[u] * (int64_t)a.deg[v];
-            double acc = 0.0;
-            for (int64_t cb = fold ? 0 : (s0 - sa) / 32; cb < nw; cb += 32) {
+            for (int64_t cb = (s0 - sa) / 32; cb < nw; cb += 32) {
                 const int64_t cc = cb + lane;
                 const uint32_t mw = cc < nw ? __ldg(a.masks + w0 + cc) : 0u;
                 unsigned nz = __ballot_sync(0xffffffffu, mw != 0u);
@@ -158,29 +150,21 @@ __global__ void __launch_bounds__(kHeavyBlock, 8) k_fill_heavy(FillArgs a, const
                             ms[q] = __shfl_sync(0xffffffffu, mw, js[q]);
                         }
                     }
-                    bool hit[Q], keep[Q];
+                    bool hit[Q];
                     int32_t z[Q], dz[Q];
 #pragma unroll
                     for (int q = 0; q < Q; ++q) {
                         const int64_t p = sa + (cb + js[q]) * 32 + lane;
-                        hit[q] = js[q] >= 0 && ((ms[q] >> lane) & 1u);
-                        keep[q] = hit[q] && p >= s0;  // before s0: z < from, for perEdge only
+                        hit[q] = js[q] >= 0 && ((ms[q] >> lane) & 1u) && p >= s0;  // before s0: z < from
                         z[q] = hit[q] ? a.nb[p] : 0;
                     }
 #pragma unroll
                     for (int q = 0; q < Q; ++q) dz[q] = hit[q] ? a.deg[z[q]] : 0;
 #pragma unroll
                     for (int q = 0; q < Q; ++q)
-                        if (js[q] >= 0) {  // uniform across the warp
-                            if (fold) {
-                                const double w = hit[q] ? 1.0 / (double)(duv * (int64_t)dz[q]) : 0.0;
-                                fold_hits(hit[q], w, s_w[wib], lane, &acc, nullptr, 0);
-                            }
-                            emit(keep[q], z[q], dz[q]);
-                        }
+                        if (js[q] >= 0) emit(hit[q], z[q], dz[q]);
                 }
             }
-            if (fold && lane == 0) a.pe[i] = acc;
         } else if (t >= 0) {
             constexpr int B = 4;  // 4 chunks per step, their lookups (then degrees) in flight together
             warp_probe_walk<B>(a.rs, t, a.nb, s0, s1, a.nb[(u_short ? v1 : u1) - 1], lane,
@@ -761,7 +745,7 @@ int count_rows(rtr_graph* g, Scratch& sc, const RowSets& rs, const int64_t* cgt,
             break;
         }
         FillArgs fa{g->offsets, g->nbors, g->esrc, g->partner, g->deg, g->fwd, m, g->tune_edge, g->tune_gallop,
-                    rs, lpos, p01[0], p01[1], e01[0], lists, moff, masks, g->pe};
+                    rs, lpos, p01[0], p01[1], e01[0], lists, moff, masks};
         ktime_begin(g, KT_TRI_FILL);
         ktime_begin(g, KT_FILL_LIGHT);
         k_fill_light<<<grid_for(m, kFillBlock), kFillBlock, 0, s>>>(fa);
